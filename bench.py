@@ -1,0 +1,266 @@
+#!/usr/bin/env python
+"""Benchmark of the fluid k-space time-stepping path on B200 (one JSON line on rank 0).
+
+Workload (N = 1): the 256^3 heterogeneous nonlinear absorbing solve (y = 1.1, BonA 5 with a
+B/A = 9 ball, 32x32 ux piston, xy-plane p + volume p_max), Nt = 1500, seeded synthetic media.
+A "step" is one time step of that simulation.  ``value`` is voxel-steps/s over K device-timed
+steps with all fields resident in HBM (CUDA events on the simulation's stream, max over ranks);
+``e2e`` is one full solve through the public API from host arrays to FP64 outputs (wall clock,
+host<->device copies inside).  Multi-GPU: every rank runs its own independent simulation
+(weak scaling; simulations shard with no collective).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c3|c2]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "k-wave-julia_b200"))
+
+# Spectral-pass-model words per voxel-step (algorithmic bytes = 4 B x words), per config.
+SPM_WORDS = {"c3": 33.0, "c2": 26.0, "c1": 15.01}
+UNIT = "Gvoxel-steps/s"
+METRIC = "Gvoxel-steps/s (fluid k-space time stepping)"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_case(name, Nt=None):
+    from kwave_b200 import workloads
+    if name == "c3":
+        return workloads.c3() if Nt is None else workloads.c3(Nt=Nt)
+    if name == "c2":
+        return workloads.c2() if Nt is None else workloads.c2(Nt=Nt)
+    if name == "c1":
+        return workloads.c1() if Nt is None else workloads.c1(Nt=Nt)
+    raise ValueError(name)
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        try:
+            self.file.seek(0)
+            rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier_max(pg, local, value):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is not None:
+        barrier_max(pg, local, 0.0)
+
+
+def cpu_baseline(case_name, budget_s=20.0):
+    """The FP64 oracle (restatement of the reference algorithm) on the host cores, a bounded
+    number of time steps of the same workload; returns voxel-steps/s and the sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _util import oracle_inputs
+    import kwave_ref as K
+    case = make_case(case_name)
+    g, m, s, sen, opts = oracle_inputs(case)
+    t0 = time.perf_counter()
+    K.kspace_first_order(g, m, s, sen, max_steps=1, **opts)  # warm-up + set-up cost
+    one = time.perf_counter() - t0
+    steps = max(2, min(case.Nt, int(budget_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    K.kspace_first_order(g, m, s, sen, max_steps=steps, **opts)
+    el = time.perf_counter() - t0
+    # subtract the per-solve set-up measured by the 1-step run's share (conservative: keep it)
+    v = case.voxels * steps / el
+    return v, steps, el, os.cpu_count()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    v, steps, el, cores = cpu_baseline(args.config, budget_s=min(60.0, 10.0 * max(1, args.steps) ** 0.5))
+    val = v / 1e9
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": make_case(args.config, Nt=2).name, "sample": f"first {steps} time steps"},
+            "impl": "reference",
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"FP64 NumPy/SciPy restatement of the reference, first {steps} "
+                                       f"time steps of the workload, scipy.fft workers={cores}"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import numpy as np
+    import kwave_b200 as kb
+
+    ctx = kb.Context(local)
+    case = make_case(args.config)
+    W = max(3, args.warmup)
+    K = max(1, min(args.steps, case.Nt - W))
+    g, m, s, sen, kw = case.to_api()
+    sim = kb.Simulation(g, m, s, sen, extra_sensors=case.extra_sensors, context=ctx, **kw)
+    info = sim.info()
+    sim.advance_timed(W)
+    barrier(pg, local)
+    with Clocks(local) as clk:
+        ms = sim.advance_timed(K)
+    ms = barrier_max(pg, local, ms)
+    sim.close()
+    vox = case.voxels
+    value = world * vox * K / (ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    spm_bytes = 4.0 * SPM_WORDS[args.config]
+    spm_frac = spm_bytes * value * 1e9 / world / (peak * 1e9)
+
+    # per-kernel device times (CUDA events around each launch on the simulation's stream)
+    prof_sim = kb.Simulation(g, m, s, sen, extra_sensors=case.extra_sensors, context=ctx, **kw)
+    prof_sim.advance(W)
+    prof = prof_sim.profile(min(20, case.Nt - W))
+    prof_sim.close()
+    tot = sum(k["total_ms"] for k in prof)
+    dom = max(prof, key=lambda k: k["total_ms"])
+    dom_avg_s = dom["total_ms"] / dom["launches"] / 1e3
+    achieved = dom["bytes_per_launch"] / dom_avg_s / 1e9
+    kernels = {k["name"]: {"avg_us": 1e3 * k["total_ms"] / k["launches"], "share": k["total_ms"] / tot,
+                           "GBps": (k["bytes_per_launch"] / (k["total_ms"] / k["launches"] / 1e3) / 1e9)
+                           if k["bytes_per_launch"] else None} for k in prof}
+
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        sim2 = kb.Simulation(g, m, s, sen, extra_sensors=case.extra_sensors, context=ctx, **kw)
+        sim2.advance(case.Nt)
+        out = sim2.outputs()
+        el = time.perf_counter() - t0
+        sim2.close()
+        h2d = sum(np.asarray(v).nbytes for v in (case.medium["sound_speed"], case.medium["density"],
+                                                 case.medium.get("BonA")) if v is not None and np.ndim(v) > 0)
+        for v in case.source.values():
+            if isinstance(v, np.ndarray) and v.dtype != bool:
+                h2d += v.astype(np.float64).nbytes
+        d2h = sum(a.nbytes for a in out.data.values()) + sum(a.nbytes for e in out.extra for a in e.values())
+        e2e = {"value": world * vox * case.Nt / el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d / case.Nt), "d2h_bytes_per_step": int(d2h / case.Nt),
+               "solve_s": el, "steps": case.Nt}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, steps, el, cores = cpu_baseline(args.config)
+        cpu = {"value": v / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"FP64 NumPy/SciPy restatement of the reference, first {steps} time steps of the "
+                         f"same workload ({el:.1f} s), scipy.fft workers={cores}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": case.name, "grid": list(case.N), "Nt": case.Nt,
+                       "l2": "inputs larger than L2 (7 FP32 state fields + medium, > 126 MB)",
+                       "timing": "CUDA events on the simulation stream, CUDA-graph replay of 32-step chunks"},
+            "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": f"{peak_kind} copy bandwidth (burst)"},
+            "spm": {"bytes_per_voxel_step": spm_bytes, "achieved_GBps": spm_bytes * value * 1e9 / world / 1e9,
+                    "frac": spm_frac},
+            "kernels": kernels,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": info["launches_per_step"] * K + (K // 32),
+        }
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1012 @@
+// C ABI of libkwb: context, validation, device admission, simulation set-up, stepping
+// (eager or CUDA-graph replay), output read-back and per-kernel profiling.
+//
+// The set-up restates the allocation and pre-computation half of kspace_first_order
+// (KWave.jl/src/solver/first_order.jl:92-441 for 1D/2D, 505-669 for 3D); the stepping restates
+// its time loop (first_order.jl:232-266, 448-484, 677-713) with the kernels of kwb_kernels.cu.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/kwb.h"
+#include "kwb_internal.h"
+
+struct kwb_ctx {
+  int device = 0;
+  std::string err;
+};
+
+static std::string g_create_err;
+static const double kPi = 3.141592653589793238462643;
+
+namespace {
+
+using namespace kwb;
+
+int set_err(kwb_ctx *ctx, int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return code;
+}
+
+#define CU(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_err(ctx, KWB_E_DEVICE, "CUDA error %s at %s:%d (%s)",                  \
+                     cudaGetErrorString(e_), __FILE__, __LINE__, #call);                \
+  } while (0)
+
+// Julia's mean() sums pairwise; a pairwise sum keeps c_ref at FP64 round-off as well.
+double pairwise_sum(const double *x, long long n) {
+  if (n <= 128) {
+    double s = 0.0;
+    for (long long i = 0; i < n; ++i) s += x[i];
+    return s;
+  }
+  const long long h = n / 2;
+  return pairwise_sum(x, h) + pairwise_sum(x + h, n - h);
+}
+
+bool make_plan(int N, FftPlan &pl) {
+  pl.n = N;
+  pl.nstages = 0;
+  int n = N, a = 0;
+  while (n % 2 == 0) {
+    n /= 2;
+    ++a;
+  }
+  while (a >= 3) {
+    pl.radix[pl.nstages++] = 8;
+    a -= 3;
+  }
+  if (a == 2) pl.radix[pl.nstages++] = 4;
+  if (a == 1) pl.radix[pl.nstages++] = 2;
+  for (int p : {3, 5, 7}) {
+    while (n % p == 0) {
+      if (pl.nstages >= KWB_MAX_STAGES) return false;
+      pl.radix[pl.nstages++] = p;
+      n /= p;
+    }
+  }
+  return n == 1;
+}
+
+int choose_L(int N, int want, int cap_lines, int dispersion, bool spec) {
+  int L = want;
+  if (L < 1) L = 1;
+  while (L > 1 && (spec ? spec_pass_smem(N, L, dispersion) : line_pass_smem(N, L)) > 200 * 1024)
+    L /= 2;
+  if (cap_lines > 0 && L > cap_lines) L = cap_lines;
+  if (L < 1) L = 1;
+  return L;
+}
+
+struct DevBuf {
+  std::vector<void *> ptrs;
+  size_t bytes = 0;
+  ~DevBuf() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  cudaError_t alloc(T **out, size_t count) {
+    void *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) return e;
+    ptrs.push_back(p);
+    bytes += count * sizeof(T);
+    *out = static_cast<T *>(p);
+    return cudaSuccess;
+  }
+};
+
+}  // namespace
+
+__global__ void kwb_k_fill_f32(float *p, long long n, float v) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+__global__ void kwb_k_fill_f64(double *p, long long n, double v) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+struct GroupHost {
+  kwb_sensor_group spec;
+  GroupDev dev{};
+  GroupDev *d_dev = nullptr;
+  long long n = 0;
+};
+
+struct kwb_sim {
+  kwb_ctx *ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  DevBuf mem;
+  SimDev h{};
+  SimDev *d_sim = nullptr;
+  long long *d_t0 = nullptr;
+  long long t0_host = 0;
+  long long Nt_loop = 0;
+  long long Nt_grid = 0;
+  long long steps_done = 0;
+  std::vector<GroupHost> groups;
+  bool tr = false;
+  kwb_progress_fn progress = nullptr;
+  void *progress_user = nullptr;
+  float *p_host = nullptr;  // pinned, progress callback
+  cudaGraphExec_t graph = nullptr;
+  int graph_K = 0;
+  int launches_per_step = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~kwb_sim() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (p_host) cudaFreeHost(p_host);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int validate_index(kwb_ctx *ctx, const int64_t *idx, int64_t n, int64_t nvox, const char *what) {
+  if (n < 0) return set_err(ctx, KWB_E_INVALID, "%s: negative point count", what);
+  if (n > 0 && !idx) return set_err(ctx, KWB_E_INVALID, "%s: index pointer is NULL", what);
+  for (int64_t i = 0; i < n; ++i) {
+    if (idx[i] < 0 || idx[i] >= nvox)
+      return set_err(ctx, KWB_E_INVALID, "%s: index %lld out of range [0, %lld)", what,
+                     (long long)idx[i], (long long)nvox);
+    if (i > 0 && idx[i] <= idx[i - 1])
+      return set_err(ctx, KWB_E_INVALID, "%s: indices must be sorted and unique", what);
+  }
+  return KWB_OK;
+}
+
+int validate_problem(kwb_ctx *ctx, const kwb_problem *P) {
+  if (!P) return set_err(ctx, KWB_E_INVALID, "problem is NULL");
+  if (P->ndim < 1 || P->ndim > 3) return set_err(ctx, KWB_E_INVALID, "ndim must be 1, 2 or 3");
+  long long nvox = 1;
+  for (int a = 0; a < 3; ++a) {
+    const int64_t n = a < P->ndim ? P->N[a] : 1;
+    if (n < 1) return set_err(ctx, KWB_E_INVALID, "grid size N[%d] = %lld must be >= 1", a, (long long)n);
+    if (n > KWB_MAX_N)
+      return set_err(ctx, KWB_E_UNSUPPORTED, "grid size N[%d] = %lld exceeds %d", a, (long long)n, KWB_MAX_N);
+    FftPlan pl;
+    if (!make_plan((int)n, pl))
+      return set_err(ctx, KWB_E_UNSUPPORTED,
+                     "grid size N[%d] = %lld has a prime factor above 7 (the FFT engine supports "
+                     "radices 2, 3, 5 and 7)", a, (long long)n);
+    if (a < P->ndim && !(P->d[a] > 0)) return set_err(ctx, KWB_E_INVALID, "grid spacing d[%d] must be > 0", a);
+    nvox *= n;
+  }
+  if (P->Nt == 0 || P->dt == 0)
+    return set_err(ctx, KWB_E_INVALID, "Time array not set. Call make_time!(kgrid, sound_speed) before running.");
+  if (P->Nt < 0 || !(P->dt > 0)) return set_err(ctx, KWB_E_INVALID, "Nt and dt must be positive");
+  for (int a = 0; a < P->ndim; ++a)
+    if (P->pml_size[a] < 0) return set_err(ctx, KWB_E_INVALID, "pml_size must be >= 0");
+  auto chk_field = [&](const kwb_field &f, const char *nm, bool optional) -> int {
+    if (f.count == 0) return optional ? KWB_OK : set_err(ctx, KWB_E_INVALID, "%s is required", nm);
+    if (!f.data) return set_err(ctx, KWB_E_INVALID, "%s: data is NULL", nm);
+    if (f.count != 1 && f.count != nvox)
+      return set_err(ctx, KWB_E_INVALID, "%s: %lld values for a grid of %lld points", nm,
+                     (long long)f.count, nvox);
+    return KWB_OK;
+  };
+  int rc;
+  if ((rc = chk_field(P->c0, "sound_speed", false))) return rc;
+  if ((rc = chk_field(P->rho0, "density", true))) return rc;
+  if ((rc = chk_field(P->BonA, "BonA", true))) return rc;
+  if (P->p0.count != 0 && (P->p0.count != nvox || !P->p0.data))
+    return set_err(ctx, KWB_E_INVALID, "p0 must have one value per grid point");
+  if (P->alpha_mode < 0 || P->alpha_mode > 2) return set_err(ctx, KWB_E_INVALID, "bad alpha_mode");
+  if ((rc = validate_index(ctx, P->p_index, P->n_p_index, nvox, "p_mask"))) return rc;
+  if ((rc = validate_index(ctx, P->u_index, P->n_u_index, nvox, "u_mask"))) return rc;
+  if (P->n_p_index > 0) {
+    if (!P->p_signal.data) return set_err(ctx, KWB_E_INVALID, "pressure source signal is NULL");
+    if (P->p_signal.n_rows < P->n_p_index || P->p_signal.n_cols < 1)
+      return set_err(ctx, KWB_E_INVALID,
+                     "BoundsError: source.p has %lld rows for %lld p_mask points",
+                     (long long)P->p_signal.n_rows, (long long)P->n_p_index);
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (!P->u_signal[d].data || P->n_u_index == 0) continue;
+    if (P->u_signal[d].n_rows < P->n_u_index || P->u_signal[d].n_cols < 1)
+      return set_err(ctx, KWB_E_INVALID, "BoundsError: velocity source %d has %lld rows for %lld u_mask points",
+                     d, (long long)P->u_signal[d].n_rows, (long long)P->n_u_index);
+  }
+  if (P->n_groups < 0 || (P->n_groups > 0 && !P->groups))
+    return set_err(ctx, KWB_E_INVALID, "sensor groups missing");
+  for (int g = 0; g < P->n_groups; ++g) {
+    const kwb_sensor_group &G = P->groups[g];
+    if (G.record_mask >> KWB_REC_COUNT) return set_err(ctx, KWB_E_INVALID, "bad record mask");
+    if (!G.dense && !G.cartesian && (rc = validate_index(ctx, G.index, G.n_index, nvox, "sensor mask")))
+      return rc;
+    if (G.dense && G.n_index != nvox && G.n_index != 0)
+      return set_err(ctx, KWB_E_INVALID, "dense sensor group must cover the grid");
+  }
+  if (P->tr.data) {
+    if (P->n_groups < 1) return set_err(ctx, KWB_E_INVALID, "time reversal needs a sensor mask");
+    const kwb_sensor_group &G = P->groups[0];
+    const long long npts = G.cartesian ? 0 : (G.dense ? nvox : G.n_index);
+    if (P->tr.n_cols < 1) return set_err(ctx, KWB_E_INVALID, "time-reversal data has no columns");
+    if (npts > 0 && P->tr.n_rows < npts)
+      return set_err(ctx, KWB_E_INVALID, "BoundsError: time-reversal data has %lld rows for %lld mask points",
+                     (long long)P->tr.n_rows, npts);
+    const uint32_t series = (1u << KWB_REC_P) | (1u << KWB_REC_UX) | (1u << KWB_REC_UY) | (1u << KWB_REC_UZ);
+    for (int g = 0; g < P->n_groups; ++g)
+      if ((P->groups[g].record_mask & series) && !P->groups[g].cartesian && P->tr.n_cols > P->Nt)
+        return set_err(ctx, KWB_E_INVALID,
+                       "BoundsError: time-series outputs have %lld columns but time reversal runs %lld steps",
+                       (long long)P->Nt, (long long)P->tr.n_cols);
+  }
+  if (P->alpha_mode != KWB_NO_ABSORPTION) {
+    if (!std::isfinite(P->alpha_coeff) || !std::isfinite(P->alpha_power))
+      return set_err(ctx, KWB_E_INVALID, "alpha_coeff and alpha_power must be set for an absorbing medium");
+  }
+  return KWB_OK;
+}
+
+void group_sizes(const kwb_problem *P, const kwb_sensor_group &G, long long nvox, kwb_group_sizes &s) {
+  for (int f = 0; f < KWB_REC_COUNT; ++f) s.rows[f] = s.cols[f] = 0;
+  const long long n = G.dense ? nvox : G.n_index;
+  for (int f = 0; f < KWB_REC_COUNT; ++f) {
+    if (!(G.record_mask & (1u << f))) continue;
+    s.rows[f] = n;
+    const bool series = f == KWB_REC_P || f == KWB_REC_UX || f == KWB_REC_UY || f == KWB_REC_UZ;
+    s.cols[f] = series ? P->Nt : 1;
+  }
+}
+
+// Point sources that fall on the lines of axis `a`: CSR over line ids.
+void build_csr(const int64_t *idx, long long n, const int N[3], int a, std::vector<int> &ptr,
+               std::vector<SrcEntry> &ent) {
+  const long long Nx = N[0], Ny = N[1], Nz = N[2];
+  const long long n_lines = a == 0 ? Ny * Nz : (a == 1 ? Nx * Nz : Nx * Ny);
+  ptr.assign(n_lines + 1, 0);
+  std::vector<SrcEntry> tmp(n);
+  for (long long j = 0; j < n; ++j) {
+    const long long v = idx[j];
+    const long long x = v % Nx, y = (v / Nx) % Ny, z = v / (Nx * Ny);
+    SrcEntry e;
+    e.line = (int)(a == 0 ? y + Ny * z : (a == 1 ? x + Nx * z : x + Nx * y));
+    e.pos = (int)(a == 0 ? x : (a == 1 ? y : z));
+    e.j = (int)j;
+    e.pad = 0;
+    tmp[j] = e;
+    ptr[e.line + 1]++;
+  }
+  for (long long l = 0; l < n_lines; ++l) ptr[l + 1] += ptr[l];
+  ent.resize(n);
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (long long j = 0; j < n; ++j) ent[fill[tmp[j].line]++] = tmp[j];
+}
+
+int upload(kwb_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return KWB_OK;
+  CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  return KWB_OK;
+}
+
+int fill_f32(kwb_ctx *ctx, float *p, long long n, float v, cudaStream_t st) {
+  if (n <= 0) return KWB_OK;
+  kwb_k_fill_f32<<<(int)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+  CU(cudaGetLastError());
+  return KWB_OK;
+}
+int fill_f64(kwb_ctx *ctx, double *p, long long n, double v, cudaStream_t st) {
+  if (n <= 0) return KWB_OK;
+  kwb_k_fill_f64<<<(int)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+  CU(cudaGetLastError());
+  return KWB_OK;
+}
+
+// Enqueue one time step (eager).  step_s is relative to the device step base.
+cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
+  const SimDev &h = S->h;
+  cudaStream_t st = S->stream;
+  cudaError_t e;
+  if (S->tr && (e = launch_tr_inject(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
+  // line passes: y, z, then x
+  for (int a : {1, 2, 0}) {
+    if (a >= h.ndim) continue;
+    if ((e = launch_line_pass(S->d_sim, h, a, KWB_MODE_STEP, step_s, st)) != cudaSuccess) return e;
+  }
+  if ((e = launch_eos_x_fwd(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
+  if (h.ndim == 2) {
+    if ((e = launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, step_s, st)) != cudaSuccess) return e;
+  } else if (h.ndim == 3) {
+    if ((e = launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD, step_s, st)) != cudaSuccess) return e;
+    if ((e = launch_spec_pass(S->d_sim, h, 2, KWB_SPEC_FWD_MUL_INV, step_s, st)) != cudaSuccess) return e;
+    if ((e = launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_INV, step_s, st)) != cudaSuccess) return e;
+  }
+  if ((e = launch_eos_x_inv(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
+  for (auto &g : S->groups) {
+    if (g.spec.cartesian || g.n == 0) continue;
+    if ((e = launch_sensor_gather(S->d_sim, h, g.d_dev, g.n, step_s, st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int count_launches(const kwb_sim *S) {
+  int n = (S->tr ? 1 : 0) + S->h.ndim + 2 + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? 3 : 0));
+  for (auto &g : S->groups)
+    if (!g.spec.cartesian && g.n > 0) ++n;
+  return n;
+}
+
+}  // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+
+extern "C" {
+
+int kwb_version(void) { return KWB_VERSION; }
+
+int kwb_context_create(int device, kwb_ctx **out) {
+  if (!out) return KWB_E_INVALID;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    g_create_err = std::string("no CUDA device available: ") + cudaGetErrorString(e);
+    return KWB_E_DEVICE;
+  }
+  if (device < 0 || device >= n) {
+    g_create_err = "device ordinal out of range";
+    return KWB_E_INVALID;
+  }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    g_create_err = cudaGetErrorString(e);
+    return KWB_E_DEVICE;
+  }
+  if (prop.major != 10) {
+    g_create_err = "libkwb is built for sm_100a (B200); device is sm_" + std::to_string(prop.major) +
+                   std::to_string(prop.minor);
+    return KWB_E_UNSUPPORTED;
+  }
+  kwb_ctx *ctx = new kwb_ctx();
+  ctx->device = device;
+  *out = ctx;
+  return KWB_OK;
+}
+
+void kwb_context_destroy(kwb_ctx *ctx) { delete ctx; }
+
+const char *kwb_last_error(const kwb_ctx *ctx) {
+  return ctx ? ctx->err.c_str() : g_create_err.c_str();
+}
+
+int kwb_query_outputs(kwb_ctx *ctx, const kwb_problem *P, kwb_group_sizes *sizes,
+                      int64_t *p_final_full_len) {
+  int rc = validate_problem(ctx, P);
+  if (rc) return rc;
+  long long nvox = 1;
+  for (int a = 0; a < P->ndim; ++a) nvox *= P->N[a];
+  for (int g = 0; g < P->n_groups; ++g) group_sizes(P, P->groups[g], nvox, sizes[g]);
+  if (p_final_full_len) *p_final_full_len = P->tr.data ? nvox : 0;
+  return KWB_OK;
+}
+
+int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
+  if (!ctx || !out) return KWB_E_INVALID;
+  *out = nullptr;
+  int rc = validate_problem(ctx, P);
+  if (rc) return rc;
+  CU(cudaSetDevice(ctx->device));
+  std::unique_ptr<kwb_sim> S(new kwb_sim());
+  S->ctx = ctx;
+  CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  CU(cudaEventCreate(&S->ev0));
+  CU(cudaEventCreate(&S->ev1));
+  cudaStream_t st = S->stream;
+  SimDev &h = S->h;
+  DevBuf &M = S->mem;
+
+  const int D = P->ndim;
+  h.ndim = D;
+  h.D = D;
+  for (int a = 0; a < 3; ++a) h.N[a] = a < D ? (int)P->N[a] : 1;
+  h.n1 = h.N[0] / 2 + 1;
+  h.nvox = (long long)h.N[0] * h.N[1] * h.N[2];
+  h.nspec = (long long)h.n1 * h.N[1] * h.N[2];
+  h.dt = (float)P->dt;
+  const long long nvox = h.nvox;
+  S->tr = P->tr.data != nullptr;
+  S->Nt_grid = P->Nt;
+  S->Nt_loop = S->tr ? P->tr.n_cols : P->Nt;
+  h.Nt = S->Nt_loop;
+
+  // ---- medium scalars / flags
+  const bool c_arr = P->c0.count == nvox && nvox > 1;
+  const bool r_arr = P->rho0.count == nvox && nvox > 1;
+  const bool b_arr = P->BonA.count == nvox && nvox > 1;
+  const double c_s = P->c0.data[0];
+  const double r_s = P->rho0.count ? P->rho0.data[0] : 1.0;
+  const double c_ref = c_arr ? pairwise_sum(P->c0.data, nvox) / (double)nvox : c_s;
+  const bool absorbing = P->alpha_mode != KWB_NO_ABSORPTION;
+  const bool nonlinear = P->BonA.count > 0;
+  h.nonlinear = nonlinear;
+  h.scalar_c = !c_arr;
+  h.dispersion = (!c_arr && absorbing && P->alpha_mode == KWB_STOKES) ? 1 : 0;
+  h.dt_over_rho0_s = (float)(P->dt / r_s);
+  h.dt_rho0_s = (float)(P->dt * r_s);
+  h.c0sq_s = (float)(c_s * c_s);
+  double tau = 0, eta = 0, y = 0;
+  if (absorbing) {
+    y = P->alpha_power;
+    const double a_np = P->alpha_coeff * (1e-2 / (20.0 * std::log10(std::exp(1.0)))) *
+                        std::pow(2.0 * kPi * 1e6, -y);
+    tau = -2.0 * a_np * std::pow(c_ref, y - 1.0);
+    eta = 2.0 * a_np * std::pow(c_ref, y - 1.0) * std::tan(kPi * y / 2.0);
+  }
+
+  // ---- tile shapes and FFT plans
+  for (int a = 0; a < 3; ++a) make_plan(h.N[a], h.plan[a]);
+  h.L_line[0] = choose_L(h.N[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, 0, false);
+  for (int a = 1; a < 3; ++a) h.L_line[a] = choose_L(h.N[a], 8, (h.N[0] + 1) / 2, 0, false);
+  h.L_eosx = choose_L(h.N[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, h.dispersion, true);
+  for (int a = 1; a < 3; ++a) h.L_spec[a] = choose_L(h.N[a], 8, h.n1, h.dispersion, true);
+  h.L_spec[0] = 1;
+
+  // ---- admission by free device memory
+  {
+    size_t need = (size_t)nvox * 4 * (1 + 2 * D) + (size_t)h.nspec * 8;
+    if (h.dispersion) need += (size_t)nvox * 4 + (size_t)h.nspec * 8;
+    need += (size_t)h.nspec * 4 * (h.dispersion ? 2 : 1);
+    need += (size_t)nvox * 4 * ((r_arr ? 1 : 0) + (c_arr ? 1 : 0) + ((nonlinear && (b_arr || r_arr)) ? 1 : 0));
+    need += (size_t)nvox * 8;  // FP64 staging for medium uploads
+    for (int g = 0; g < P->n_groups; ++g) {
+      const kwb_sensor_group &G = P->groups[g];
+      if (G.cartesian) continue;
+      const long long n = G.dense ? nvox : G.n_index;
+      for (int f = 0; f < KWB_REC_COUNT; ++f)
+        if (G.record_mask & (1u << f)) {
+          const bool series = f == KWB_REC_P || f == KWB_REC_UX || f == KWB_REC_UY || f == KWB_REC_UZ;
+          need += (size_t)n * (series ? (size_t)P->Nt * 4 : 8);
+        }
+    }
+    size_t free_b = 0, total_b = 0;
+    CU(cudaMemGetInfo(&free_b, &total_b));
+    if (need + (size_t)64 * 1024 * 1024 > free_b)
+      return set_err(ctx, KWB_E_NOMEM, "simulation needs %.1f MB of device memory, %.1f MB free",
+                     need / 1e6, free_b / 1e6);
+  }
+
+  // ---- fields
+  CU(M.alloc(&h.p, nvox));
+  CU(cudaMemsetAsync(h.p, 0, nvox * 4, st));
+  for (int d = 0; d < D; ++d) {
+    CU(M.alloc(&h.u[d], nvox));
+    CU(M.alloc(&h.rho[d], nvox));
+    CU(cudaMemsetAsync(h.u[d], 0, nvox * 4, st));
+    CU(cudaMemsetAsync(h.rho[d], 0, nvox * 4, st));
+  }
+  CU(M.alloc(&h.spec, h.nspec));
+  if (h.dispersion) {
+    CU(M.alloc(&h.spec2, h.nspec));
+    CU(M.alloc(&h.rho_prev, nvox));
+    CU(cudaMemsetAsync(h.rho_prev, 0, nvox * 4, st));
+  }
+  CU(M.alloc(&S->d_t0, 1));
+  CU(cudaMemsetAsync(S->d_t0, 0, 8, st));
+  h.t0 = S->d_t0;
+
+  // ---- medium (FP64 upload, FP32 on device)
+  double *stage = nullptr;
+  const bool need_stage = c_arr || r_arr || b_arr || P->p0.count;
+  if (need_stage) CU(M.alloc(&stage, nvox));
+  double *stage2 = nullptr;
+  if (nonlinear && b_arr && r_arr) CU(M.alloc(&stage2, nvox));
+  if (c_arr) {
+    float *c0sq;
+    CU(M.alloc(&c0sq, nvox));
+    if ((rc = upload(ctx, stage, P->c0.data, nvox * 8, st))) return rc;
+    CU(convert_f64_to_f32(c0sq, stage, nvox, 1, st));
+    h.c0sq = c0sq;
+  }
+  if (r_arr) {
+    float *rho0;
+    CU(M.alloc(&rho0, nvox));
+    if ((rc = upload(ctx, stage, P->rho0.data, nvox * 8, st))) return rc;
+    CU(convert_f64_to_f32(rho0, stage, nvox, 0, st));
+    h.rho0 = rho0;
+  }
+  if (nonlinear) {
+    const double b_s = P->BonA.data[0];
+    if (b_arr || r_arr) {
+      float *q;
+      CU(M.alloc(&q, nvox));
+      const double *bp = nullptr, *rp = nullptr;
+      if (b_arr && r_arr) {
+        if ((rc = upload(ctx, stage, P->BonA.data, nvox * 8, st))) return rc;
+        if ((rc = upload(ctx, stage2, P->rho0.data, nvox * 8, st))) return rc;
+        bp = stage;
+        rp = stage2;
+      } else if (b_arr) {
+        if ((rc = upload(ctx, stage, P->BonA.data, nvox * 8, st))) return rc;
+        bp = stage;
+      } else {
+        if ((rc = upload(ctx, stage, P->rho0.data, nvox * 8, st))) return rc;
+        rp = stage;
+      }
+      CU(build_nlq(q, bp, b_arr, b_s, rp, r_arr, r_s, nvox, st));
+      h.nlq = q;
+    } else {
+      h.nlq_s = (float)((b_s / 2.0) / r_s);
+    }
+  }
+
+  // ---- per-axis tables (FP64 on device)
+  for (int a = 0; a < 3; ++a) {
+    const int n = h.N[a];
+    float2 *tw, *gp, *gn;
+    float *pd, *psd;
+    CU(M.alloc(&tw, n));
+    CU(M.alloc(&gp, n));
+    CU(M.alloc(&gn, n));
+    CU(M.alloc(&pd, n));
+    CU(M.alloc(&psd, n));
+    CU(build_twiddles(tw, n, st));
+    const double d = a < D ? P->d[a] : 1.0;
+    CU(build_gradient(gp, gn, n, d, st));
+    const int psz = a < D ? (int)P->pml_size[a] : 0;
+    const double pal = a < D ? P->pml_alpha[a] : 0.0;
+    CU(build_pml_deficit(pd, n, psz, pal, P->dt, 0, st));
+    CU(build_pml_deficit(psd, n, psz, pal, P->dt, 1, st));
+    h.tw[a] = tw;
+    h.gpos[a] = gp;
+    h.gneg[a] = gn;
+    h.pml_def[a] = pd;
+    h.pml_sg_def[a] = psd;
+  }
+  {
+    float *Mt, *M2 = nullptr;
+    CU(M.alloc(&Mt, h.nspec));
+    if (h.dispersion) CU(M.alloc(&M2, h.nspec));
+    const double d3[3] = {P->d[0], D > 1 ? P->d[1] : 1.0, D > 2 ? P->d[2] : 1.0};
+    CU(build_eos_multiplier(Mt, M2, h.N, d3, c_ref, P->dt, c_arr ? 1.0 : c_s * c_s, absorbing, tau,
+                            eta, y, st));
+    h.M = Mt;
+    h.M2 = M2;
+  }
+
+  // ---- sources
+  auto c_at_points = [&](const int64_t *idx, long long n, double **dev_out) -> int {
+    *dev_out = nullptr;
+    if (!c_arr || n == 0) return KWB_OK;
+    std::vector<double> c(n);
+    for (long long j = 0; j < n; ++j) c[j] = P->c0.data[idx[j]];
+    double *dc;
+    CU(M.alloc(&dc, n));
+    if (int r = upload(ctx, dc, c.data(), n * 8, st)) return r;
+    CU(cudaStreamSynchronize(st));
+    *dev_out = dc;
+    return KWB_OK;
+  };
+  if (P->n_p_index > 0) {
+    const long long n = P->n_p_index;
+    h.n_p = (int)n;
+    h.p_mode = P->p_mode;
+    h.p_cols = (int)P->p_signal.n_cols;
+    double *sig;
+    CU(M.alloc(&sig, P->p_signal.n_rows * P->p_signal.n_cols));
+    if ((rc = upload(ctx, sig, P->p_signal.data, P->p_signal.n_rows * P->p_signal.n_cols * 8, st))) return rc;
+    double *cat;
+    if ((rc = c_at_points(P->p_index, n, &cat))) return rc;
+    float *tab;
+    CU(M.alloc(&tab, n * h.p_cols));
+    CU(build_source_table(tab, sig, P->p_signal.n_rows, n, h.p_cols, cat, c_s, c_arr, (double)D, 1, st));
+    h.p_sig = tab;
+    for (int a = 0; a < D; ++a) {
+      std::vector<int> ptr;
+      std::vector<SrcEntry> ent;
+      build_csr(P->p_index, n, h.N, a, ptr, ent);
+      int *dptr;
+      SrcEntry *dent;
+      CU(M.alloc(&dptr, ptr.size()));
+      CU(M.alloc(&dent, ent.size()));
+      if ((rc = upload(ctx, dptr, ptr.data(), ptr.size() * 4, st))) return rc;
+      if ((rc = upload(ctx, dent, ent.data(), ent.size() * sizeof(SrcEntry), st))) return rc;
+      CU(cudaStreamSynchronize(st));
+      h.p_line_ptr[a] = dptr;
+      h.p_entry[a] = dent;
+    }
+  }
+  if (P->n_u_index > 0) {
+    const long long n = P->n_u_index;
+    h.n_u = (int)n;
+    h.u_mode = P->u_mode;
+    for (int a = 0; a < D; ++a) {
+      const kwb_signal &sg = P->u_signal[a];
+      if (!sg.data) continue;
+      h.u_cols[a] = (int)sg.n_cols;
+      double *sig;
+      CU(M.alloc(&sig, sg.n_rows * sg.n_cols));
+      if ((rc = upload(ctx, sig, sg.data, sg.n_rows * sg.n_cols * 8, st))) return rc;
+      float *tab;
+      CU(M.alloc(&tab, n * sg.n_cols));
+      CU(build_source_table(tab, sig, sg.n_rows, n, sg.n_cols, nullptr, 1.0, 0, 1.0, 0, st));
+      h.u_sig[a] = tab;
+      std::vector<int> ptr;
+      std::vector<SrcEntry> ent;
+      build_csr(P->u_index, n, h.N, a, ptr, ent);
+      int *dptr;
+      SrcEntry *dent;
+      CU(M.alloc(&dptr, ptr.size()));
+      CU(M.alloc(&dent, ent.size()));
+      if ((rc = upload(ctx, dptr, ptr.data(), ptr.size() * 4, st))) return rc;
+      if ((rc = upload(ctx, dent, ent.data(), ent.size() * sizeof(SrcEntry), st))) return rc;
+      CU(cudaStreamSynchronize(st));
+      h.u_line_ptr[a] = dptr;
+      h.u_entry[a] = dent;
+    }
+  }
+
+  // ---- sensor groups
+  S->groups.resize(P->n_groups);
+  for (int g = 0; g < P->n_groups; ++g) {
+    GroupHost &G = S->groups[g];
+    G.spec = P->groups[g];
+    G.spec.index = nullptr;
+    if (G.spec.cartesian) continue;
+    const kwb_sensor_group &in = P->groups[g];
+    G.n = in.dense ? nvox : in.n_index;
+    GroupDev &gd = G.dev;
+    gd.n = G.n;
+    gd.dense = in.dense;
+    gd.mask = in.record_mask;
+    gd.cnt_prms = std::max<int>(1, in.record_count[KWB_REC_P_RMS]);
+    gd.cnt_urms = std::max<int>(1, in.record_count[KWB_REC_U_RMS]);
+    gd.cnt_iavg = std::max<int>(1, in.record_count[KWB_REC_I_AVG]);
+    gd.nt_alloc = P->Nt;
+    if (G.n == 0) continue;
+    if (!in.dense) {
+      long long *di;
+      CU(M.alloc(&di, G.n));
+      if ((rc = upload(ctx, di, in.index, G.n * 8, st))) return rc;
+      CU(cudaStreamSynchronize(st));
+      gd.idx = di;
+    }
+    const unsigned m = in.record_mask;
+    if (m & (1u << KWB_REC_P)) {
+      CU(M.alloc(&gd.ser_p, G.n * P->Nt));
+      CU(cudaMemsetAsync(gd.ser_p, 0, G.n * P->Nt * 4, st));
+    }
+    for (int d = 0; d < 3; ++d)
+      if (m & (1u << (KWB_REC_UX + d))) {
+        CU(M.alloc(&gd.ser_u[d], G.n * P->Nt));
+        CU(cudaMemsetAsync(gd.ser_u[d], 0, G.n * P->Nt * 4, st));
+      }
+    if (m & (1u << KWB_REC_P_MAX)) { CU(M.alloc(&gd.pmax, G.n)); if ((rc = fill_f32(ctx, gd.pmax, G.n, -INFINITY, st))) return rc; }
+    if (m & (1u << KWB_REC_P_MIN)) { CU(M.alloc(&gd.pmin, G.n)); if ((rc = fill_f32(ctx, gd.pmin, G.n, INFINITY, st))) return rc; }
+    if (m & (1u << KWB_REC_P_FINAL)) { CU(M.alloc(&gd.pfinal, G.n)); if ((rc = fill_f32(ctx, gd.pfinal, G.n, 0.f, st))) return rc; }
+    if (m & (1u << KWB_REC_P_RMS)) { CU(M.alloc(&gd.prms, G.n)); if ((rc = fill_f64(ctx, gd.prms, G.n, 0.0, st))) return rc; }
+    if (m & (1u << KWB_REC_U_MAX)) { CU(M.alloc(&gd.umax, G.n)); if ((rc = fill_f64(ctx, gd.umax, G.n, -INFINITY, st))) return rc; }
+    if (m & (1u << KWB_REC_U_RMS)) { CU(M.alloc(&gd.urms, G.n)); if ((rc = fill_f64(ctx, gd.urms, G.n, 0.0, st))) return rc; }
+    if (m & (1u << KWB_REC_U_FINAL)) { CU(M.alloc(&gd.ufinal, G.n)); if ((rc = fill_f64(ctx, gd.ufinal, G.n, 0.0, st))) return rc; }
+    if (m & (1u << KWB_REC_I_AVG)) { CU(M.alloc(&gd.iavg, G.n)); if ((rc = fill_f64(ctx, gd.iavg, G.n, 0.0, st))) return rc; }
+    if (m & (1u << KWB_REC_I_MAX)) { CU(M.alloc(&gd.imax, G.n)); if ((rc = fill_f64(ctx, gd.imax, G.n, -INFINITY, st))) return rc; }
+    CU(M.alloc(&G.d_dev, 1));
+    if ((rc = upload(ctx, G.d_dev, &gd, sizeof(GroupDev), st))) return rc;
+    CU(cudaStreamSynchronize(st));
+  }
+
+  // ---- time reversal data: p / (D c^2) at group 0's points
+  if (S->tr) {
+    const kwb_sensor_group &G0 = P->groups[0];
+    const long long n = G0.cartesian ? 0 : (G0.dense ? nvox : G0.n_index);
+    h.n_tr = (int)n;
+    if (n > 0) {
+      std::vector<int64_t> idx;
+      const int64_t *ip = G0.index;
+      if (G0.dense) {
+        idx.resize(n);
+        for (long long j = 0; j < n; ++j) idx[j] = j;
+        ip = idx.data();
+      }
+      long long *di;
+      CU(M.alloc(&di, n));
+      if ((rc = upload(ctx, di, ip, n * 8, st))) return rc;
+      double *sig;
+      CU(M.alloc(&sig, P->tr.n_rows * P->tr.n_cols));
+      if ((rc = upload(ctx, sig, P->tr.data, P->tr.n_rows * P->tr.n_cols * 8, st))) return rc;
+      double *cat;
+      if ((rc = c_at_points(ip, n, &cat))) return rc;
+      float *tab;
+      CU(M.alloc(&tab, n * P->tr.n_cols));
+      CU(build_source_table(tab, sig, P->tr.n_rows, n, P->tr.n_cols, cat, c_s, c_arr, (double)D, 1, st));
+      h.tr_idx = di;
+      h.tr_sig = tab;
+      CU(cudaStreamSynchronize(st));
+    }
+  }
+
+  CU(prime_attributes(h));
+
+  // ---- device descriptor
+  CU(M.alloc(&S->d_sim, 1));
+  if ((rc = upload(ctx, S->d_sim, &h, sizeof(SimDev), st))) return rc;
+
+  // ---- p0 initialisation (first_order_steps.jl:58-191); skipped in time-reversal mode
+  if (P->p0.count && !S->tr) {
+    if ((rc = upload(ctx, stage, P->p0.data, nvox * 8, st))) return rc;
+    CU(convert_f64_to_f32(h.p, stage, nvox, 0, st));
+    for (int a = 0; a < D; ++a) CU(launch_line_pass(S->d_sim, h, a, KWB_MODE_INIT, 0, st));
+  }
+  CU(cudaStreamSynchronize(st));
+
+  S->progress = P->progress;
+  S->progress_user = P->progress_user;
+  if (S->progress) CU(cudaMallocHost(&S->p_host, nvox * 4));
+  S->launches_per_step = count_launches(S.get());
+  *out = S.release();
+  return KWB_OK;
+}
+
+static int sim_enqueue(kwb_sim *S, long long steps) {
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaSetDevice(ctx->device));
+  const long long remaining = S->Nt_loop - S->steps_done;
+  if (steps > remaining) steps = remaining;
+  if (steps <= 0) return KWB_OK;
+  if (S->progress) {
+    for (long long i = 0; i < steps; ++i) {
+      const long long t = S->steps_done;
+      CU(enqueue_step(S, t - S->t0_host));
+      CU(cudaMemcpyAsync(S->p_host, S->h.p, S->h.nvox * 4, cudaMemcpyDeviceToHost, S->stream));
+      CU(cudaStreamSynchronize(S->stream));
+      S->steps_done++;
+      S->progress(t + 1, S->Nt_loop, S->p_host, S->progress_user);
+    }
+    return KWB_OK;
+  }
+  const int K = 32;
+  if (steps >= K && !S->graph) {
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < K && e == cudaSuccess; ++s) e = enqueue_step(S, s);
+    if (e == cudaSuccess) e = launch_advance_t0(S->d_t0, K, S->stream);
+    cudaError_t e2 = cudaStreamEndCapture(S->stream, &g);
+    if (e != cudaSuccess) return set_err(ctx, KWB_E_DEVICE, "graph capture: %s", cudaGetErrorString(e));
+    CU(e2);
+    e = cudaGraphInstantiate(&S->graph, g, 0);
+    cudaGraphDestroy(g);
+    CU(e);
+    S->graph_K = K;
+  }
+  while (S->graph && steps >= S->graph_K) {
+    CU(cudaGraphLaunch(S->graph, S->stream));
+    S->t0_host += S->graph_K;
+    S->steps_done += S->graph_K;
+    steps -= S->graph_K;
+  }
+  for (long long i = 0; i < steps; ++i) {
+    CU(enqueue_step(S, S->steps_done - S->t0_host));
+    S->steps_done++;
+  }
+  return KWB_OK;
+}
+
+int kwb_sim_advance(kwb_sim *S, int64_t steps) {
+  if (!S) return KWB_E_INVALID;
+  return sim_enqueue(S, steps);
+}
+
+int kwb_sim_advance_timed(kwb_sim *S, int64_t steps, double *device_ms) {
+  if (!S) return KWB_E_INVALID;
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaSetDevice(ctx->device));
+  CU(cudaEventRecord(S->ev0, S->stream));
+  int rc = sim_enqueue(S, steps);
+  if (rc) return rc;
+  CU(cudaEventRecord(S->ev1, S->stream));
+  CU(cudaEventSynchronize(S->ev1));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+  if (device_ms) *device_ms = ms;
+  return KWB_OK;
+}
+
+int64_t kwb_sim_steps_done(const kwb_sim *S) { return S ? S->steps_done : -1; }
+
+int kwb_sim_sync(kwb_sim *S) {
+  if (!S) return KWB_E_INVALID;
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaStreamSynchronize(S->stream));
+  return KWB_OK;
+}
+
+int kwb_sim_read_pressure(kwb_sim *S, float *p_host) {
+  if (!S || !p_host) return KWB_E_INVALID;
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaSetDevice(ctx->device));
+  CU(cudaMemcpyAsync(p_host, S->h.p, S->h.nvox * 4, cudaMemcpyDeviceToHost, S->stream));
+  CU(cudaStreamSynchronize(S->stream));
+  return KWB_OK;
+}
+
+int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
+  if (!S || !out) return KWB_E_INVALID;
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaSetDevice(ctx->device));
+  CU(cudaStreamSynchronize(S->stream));
+  const double Ntd = (double)S->Nt_loop;
+  std::vector<float> f32;
+  std::vector<double> f64;
+  for (size_t g = 0; g < S->groups.size(); ++g) {
+    if (!out->groups) break;
+    const GroupHost &G = S->groups[g];
+    kwb_group_outputs &o = out->groups[g];
+    const unsigned m = G.spec.record_mask;
+    const long long n = G.spec.cartesian ? G.spec.n_index : G.n;
+    auto want = [&](int f) { return (m & (1u << f)) && o.field[f]; };
+    if (G.spec.cartesian || n == 0) {
+      // never filled: initial values (first_order.jl:417-421, sensor.jl:109-133)
+      for (int f = 0; f < KWB_REC_COUNT; ++f) {
+        if (!want(f)) continue;
+        const bool series = f == KWB_REC_P || f == KWB_REC_UX || f == KWB_REC_UY || f == KWB_REC_UZ;
+        const long long cnt = series ? n * S->Nt_grid : n;
+        double v = 0.0;
+        if (f == KWB_REC_P_MAX || f == KWB_REC_U_MAX || f == KWB_REC_I_MAX) v = -INFINITY;
+        if (f == KWB_REC_P_MIN) v = INFINITY;
+        for (long long i = 0; i < cnt; ++i) o.field[f][i] = v;
+      }
+      continue;
+    }
+    const GroupDev &gd = G.dev;
+    auto get32 = [&](const float *src, long long cnt, double *dst) -> int {
+      f32.resize(cnt);
+      CU(cudaMemcpy(f32.data(), src, cnt * 4, cudaMemcpyDeviceToHost));
+      for (long long i = 0; i < cnt; ++i) dst[i] = (double)f32[i];
+      return KWB_OK;
+    };
+    auto get64 = [&](const double *src, long long cnt, double *dst) -> int {
+      CU(cudaMemcpy(dst, src, cnt * 8, cudaMemcpyDeviceToHost));
+      return KWB_OK;
+    };
+    int rc;
+    if (want(KWB_REC_P) && (rc = get32(gd.ser_p, n * gd.nt_alloc, o.field[KWB_REC_P]))) return rc;
+    for (int d = 0; d < 3; ++d)
+      if (want(KWB_REC_UX + d) && (rc = get32(gd.ser_u[d], n * gd.nt_alloc, o.field[KWB_REC_UX + d]))) return rc;
+    if (want(KWB_REC_P_MAX) && (rc = get32(gd.pmax, n, o.field[KWB_REC_P_MAX]))) return rc;
+    if (want(KWB_REC_P_MIN) && (rc = get32(gd.pmin, n, o.field[KWB_REC_P_MIN]))) return rc;
+    if (want(KWB_REC_P_FINAL) && (rc = get32(gd.pfinal, n, o.field[KWB_REC_P_FINAL]))) return rc;
+    if (want(KWB_REC_P_RMS)) {
+      if ((rc = get64(gd.prms, n, o.field[KWB_REC_P_RMS]))) return rc;
+      for (long long i = 0; i < n; ++i) o.field[KWB_REC_P_RMS][i] = std::sqrt(o.field[KWB_REC_P_RMS][i] / Ntd);
+    }
+    if (want(KWB_REC_U_MAX) && (rc = get64(gd.umax, n, o.field[KWB_REC_U_MAX]))) return rc;
+    if (want(KWB_REC_U_RMS)) {
+      if ((rc = get64(gd.urms, n, o.field[KWB_REC_U_RMS]))) return rc;
+      for (long long i = 0; i < n; ++i) o.field[KWB_REC_U_RMS][i] = std::sqrt(o.field[KWB_REC_U_RMS][i] / Ntd);
+    }
+    if (want(KWB_REC_U_FINAL) && (rc = get64(gd.ufinal, n, o.field[KWB_REC_U_FINAL]))) return rc;
+    if (want(KWB_REC_I_AVG) && (rc = get64(gd.iavg, n, o.field[KWB_REC_I_AVG]))) return rc;
+    if (want(KWB_REC_I_MAX) && (rc = get64(gd.imax, n, o.field[KWB_REC_I_MAX]))) return rc;
+  }
+  if (S->tr && out->p_final_full) {
+    f32.resize(S->h.nvox);
+    CU(cudaMemcpy(f32.data(), S->h.p, S->h.nvox * 4, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < S->h.nvox; ++i) out->p_final_full[i] = (double)f32[i];
+  }
+  return KWB_OK;
+}
+
+void kwb_sim_destroy(kwb_sim *S) {
+  if (!S) return;
+  cudaSetDevice(S->ctx->device);
+  if (S->stream) cudaStreamSynchronize(S->stream);
+  delete S;
+}
+
+int kwb_sim_info(const kwb_sim *S, int64_t *device_bytes, int32_t *launches_per_step) {
+  if (!S) return KWB_E_INVALID;
+  if (device_bytes) *device_bytes = (int64_t)S->mem.bytes;
+  if (launches_per_step) *launches_per_step = S->launches_per_step;
+  return KWB_OK;
+}
+
+int kwb_solve(kwb_ctx *ctx, const kwb_problem *P, kwb_outputs *out) {
+  kwb_sim *S = nullptr;
+  int rc = kwb_sim_create(ctx, P, &S);
+  if (rc) return rc;
+  rc = kwb_sim_advance(S, S->Nt_loop);
+  if (!rc) rc = kwb_sim_read_outputs(S, out);
+  kwb_sim_destroy(S);
+  return rc;
+}
+
+int kwb_sim_profile(kwb_sim *S, int64_t steps, kwb_kernel_times *out) {
+  if (!S || !out) return KWB_E_INVALID;
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaSetDevice(ctx->device));
+  memset(out, 0, sizeof(*out));
+  const SimDev &h = S->h;
+  cudaStream_t st = S->stream;
+  const double nv = (double)h.nvox, ns = (double)h.nspec;
+  const int hr = h.rho0 ? 1 : 0;
+  auto slot = [&](const char *name, double bytes) -> int {
+    for (int i = 0; i < out->n; ++i)
+      if (!strcmp(out->name[i], name)) return i;
+    const int i = out->n++;
+    snprintf(out->name[i], sizeof(out->name[i]), "%s", name);
+    out->bytes_per_launch[i] = bytes;
+    return i;
+  };
+  const long long remaining = S->Nt_loop - S->steps_done;
+  if (steps > remaining) steps = remaining;
+  std::vector<cudaEvent_t> evs;
+  struct Rec { int slot; size_t e0; };
+  std::vector<Rec> recs;
+  auto ev = [&]() -> cudaEvent_t {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    evs.push_back(e);
+    return e;
+  };
+  cudaError_t err = cudaSuccess;
+  auto timed = [&](int sl, auto fn) {
+    if (err != cudaSuccess) return;
+    cudaEvent_t a = ev(), b = ev();
+    cudaEventRecord(a, st);
+    err = fn();
+    cudaEventRecord(b, st);
+    recs.push_back({sl, evs.size() - 2});
+  };
+  for (long long i = 0; i < steps && err == cudaSuccess; ++i) {
+    const long long s = S->steps_done - S->t0_host;
+    if (S->tr) timed(slot("tr_inject", h.n_tr * 8.0), [&] { return launch_tr_inject(S->d_sim, h, s, st); });
+    for (int a : {1, 2, 0}) {
+      if (a >= h.ndim) continue;
+      static const char *nm[3] = {"line_pass_x", "line_pass_y", "line_pass_z"};
+      timed(slot(nm[a], nv * 4.0 * (5 + hr)), [&] { return launch_line_pass(S->d_sim, h, a, KWB_MODE_STEP, s, st); });
+    }
+    {
+      const double rd = nv * 4.0 * (h.D + (h.c0sq ? 1 : 0) + (h.nonlinear && h.nlq ? 1 : 0) + (h.dispersion ? 2 : 0));
+      timed(slot("eos_x_fwd", rd + ns * 8.0 * (h.dispersion ? 2 : 1)), [&] { return launch_eos_x_fwd(S->d_sim, h, s, st); });
+    }
+    if (h.ndim == 2) {
+      timed(slot("spec_y_mul", ns * 8.0 * (h.dispersion ? 3 : 2) + ns * 4.0 * (h.dispersion ? 2 : 1)),
+            [&] { return launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, s, st); });
+    } else if (h.ndim == 3) {
+      timed(slot("spec_y_fwd", ns * 16.0 * (h.dispersion ? 2 : 1)), [&] { return launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD, s, st); });
+      timed(slot("spec_z_mul", ns * 8.0 * (h.dispersion ? 3 : 2) + ns * 4.0 * (h.dispersion ? 2 : 1)),
+            [&] { return launch_spec_pass(S->d_sim, h, 2, KWB_SPEC_FWD_MUL_INV, s, st); });
+      timed(slot("spec_y_inv", ns * 16.0), [&] { return launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_INV, s, st); });
+    }
+    timed(slot("eos_x_inv", ns * 8.0 + nv * 4.0 + (h.ndim == 1 ? ns * 4.0 : 0.0)), [&] { return launch_eos_x_inv(S->d_sim, h, s, st); });
+    for (auto &g : S->groups) {
+      if (g.spec.cartesian || g.n == 0) continue;
+      timed(slot("sensor_gather", 0.0), [&] { return launch_sensor_gather(S->d_sim, h, g.d_dev, g.n, s, st); });
+    }
+    S->steps_done++;
+  }
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  for (auto &r : recs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, evs[r.e0], evs[r.e0 + 1]);
+    out->total_ms[r.slot] += ms;
+    out->launches[r.slot] += 1;
+  }
+  for (auto e : evs) cudaEventDestroy(e);
+  CU(err);
+  CU(e2);
+  return KWB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+// Internal device/host structures of libkwb (not part of the C ABI).
+//
+// Data layout in HBM (one simulation):
+//   * real fields p, u_d, rho_d (FP32): [Nz][Ny][Nx], x fastest -- the reference's column-major
+//     order, so a Julia linear index is a direct offset;
+//   * EOS half spectrum (complex FP32): [Nz][Ny][n1], n1 = Nx/2 + 1 -- the shape of the
+//     reference's rfft scratch (fft_utils.jl:178);
+//   * medium (FP32): rho0, c0^2, Q = BonA/(2 rho0), each present only when it varies per voxel;
+//   * operator tables (built in FP64 on the device, stored FP32): per-axis twiddles, gradient
+//     multipliers i k e^{+-i k d/2}/N, PML deficits 1 - pml, and the EOS multiplier
+//     M = [c^2] kappa (1 + nabla1) / (Nx Ny Nz) in the half-spectrum shape.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define KWB_MAX_STAGES 16
+#define KWB_THREADS 256
+#define KWB_MAX_N 4096
+
+struct FftPlan {
+  int n;
+  int nstages;
+  int radix[KWB_MAX_STAGES];
+};
+
+// Line-pass modes.
+enum { KWB_MODE_STEP = 0, KWB_MODE_INIT = 1 };
+// Spectrum-pass operations.
+enum { KWB_SPEC_FWD = 0, KWB_SPEC_FWD_MUL_INV = 1, KWB_SPEC_INV = 2 };
+
+// One point source that lies on a line of an axis pass: line id, position along the line,
+// source row j.
+struct SrcEntry {
+  int line;
+  int pos;
+  int j;
+  int pad;
+};
+
+struct SimDev {
+  int ndim;
+  int N[3];
+  int n1;
+  long long nvox;
+  long long nspec;
+  float dt;
+  float dt_over_rho0_s;  // dt / rho0 for scalar density
+  float dt_rho0_s;       // dt * rho0 for scalar density
+  int D;                 // number of split density components (= ndim)
+
+  float *p;
+  float *u[3];
+  float *rho[3];
+  float *rho_prev;  // dispersion only
+  float2 *spec;
+  float2 *spec2;    // dispersion only
+
+  const float *rho0;  // nullptr: scalar density
+  const float *c0sq;  // nullptr: scalar sound speed
+  float c0sq_s;
+  const float *nlq;   // nullptr: scalar Q (nlq_s)
+  float nlq_s;
+  int nonlinear;
+  int dispersion;     // scalar c0 with :stokes absorption -> second spectrum
+  int scalar_c;       // c^2 folded into M (scalar c0) vs applied per voxel
+  const float *M;     // [Nz][Ny][n1]
+  const float *M2;    // dispersion multiplier, [Nz][Ny][n1]
+
+  const float *pml_def[3];
+  const float *pml_sg_def[3];
+  const float2 *gpos[3];
+  const float2 *gneg[3];
+  const float2 *tw[3];
+  FftPlan plan[3];
+
+  // tile shapes: complex lines per tile for line passes (per axis), x-direction EOS passes and
+  // spectrum passes (per axis); tiles per plane for each
+  int L_line[3];
+  int L_eosx;
+  int L_spec[3];
+
+  // sources
+  int p_mode;
+  int n_p;
+  int p_cols;
+  const float *p_sig;  // [col][j], already divided by D c^2 at the source point
+  const int *p_line_ptr[3];
+  const SrcEntry *p_entry[3];
+  int u_mode;
+  int n_u;
+  int u_cols[3];
+  const float *u_sig[3];  // [col][j], nullptr when the component is absent
+  const int *u_line_ptr[3];
+  const SrcEntry *u_entry[3];
+
+  // time reversal
+  int n_tr;
+  const long long *tr_idx;
+  const float *tr_sig;  // [col][j] already divided by D c^2
+
+  long long Nt;
+  const long long *t0;  // device step base (CUDA graph replays advance it)
+};
+
+// Sensor group on the device.
+struct GroupDev {
+  const long long *idx;  // nullptr when dense
+  long long n;
+  int dense;
+  unsigned mask;
+  int cnt_prms, cnt_urms, cnt_iavg;
+  float *ser_p;
+  float *ser_u[3];
+  long long nt_alloc;
+  float *pmax, *pmin, *pfinal;
+  double *prms;
+  double *umax, *urms, *ufinal, *iavg, *imax;
+};
+
+// Kernel launchers (kwb_kernels.cu).
+namespace kwb {
+size_t line_pass_smem(int N, int L);
+size_t spec_pass_smem(int N, int L, int dispersion);
+cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
+                             long long step_s, cudaStream_t st);
+cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long step_s,
+                             cudaStream_t st);
+cudaError_t launch_spec_pass(const SimDev *d_sim, const SimDev &h, int axis, int op,
+                             long long step_s, cudaStream_t st);
+cudaError_t launch_eos_x_inv(const SimDev *d_sim, const SimDev &h, long long step_s,
+                             cudaStream_t st);
+cudaError_t launch_tr_inject(const SimDev *d_sim, const SimDev &h, long long step_s,
+                             cudaStream_t st);
+cudaError_t launch_sensor_gather(const SimDev *d_sim, const SimDev &h, const GroupDev *d_group,
+                                 long long n, long long step_s, cudaStream_t st);
+cudaError_t launch_advance_t0(long long *t0, long long k, cudaStream_t st);
+// Raise the dynamic shared-memory limit of every time-step kernel for this simulation's tiles.
+cudaError_t prime_attributes(const SimDev &h);
+
+// FP64 table builders.
+cudaError_t build_twiddles(float2 *out, int N, cudaStream_t st);
+cudaError_t build_gradient(float2 *pos, float2 *neg, int N, double d, cudaStream_t st);
+cudaError_t build_pml_deficit(float *out, int N, int pml_size, double alpha, double dt,
+                              int staggered, cudaStream_t st);
+cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const double d[3],
+                                 double c_ref, double dt, double c_sq_fold, int absorbing,
+                                 double tau, double eta, double y, cudaStream_t st);
+cudaError_t convert_f64_to_f32(float *out, const double *in, long long n, int op,
+                               cudaStream_t st);
+cudaError_t build_nlq(float *out, const double *bona, int bona_array, double bona_s,
+                      const double *rho0, int rho0_array, double rho0_s, long long n,
+                      cudaStream_t st);
+cudaError_t build_source_table(float *out, const double *sig, long long n_rows, long long n_pts,
+                               long long n_cols, const double *c_at_pts, double c_s,
+                               int c_array, double divisor, int apply_c, cudaStream_t st);
+}  // namespace kwb

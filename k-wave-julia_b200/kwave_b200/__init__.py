@@ -1,0 +1,24 @@
+"""kwave_b200 -- KWave.jl's fluid k-space time-stepping path on NVIDIA B200 (sm_100a).
+
+The user-facing names mirror KWave.jl (KWave.jl/src/KWave.jl exports): build a grid, medium,
+source and sensor, then call ``kspace_first_order``.  The time loop runs in libkwb.so
+(hand-written CUDA, C ABI in include/kwb.h); there is no CPU fallback.
+"""
+
+from .core import (Additive, AdditiveNoCorrection, Dirichlet, KWaveGrid, KWaveMedium, KWaveSensor,
+                   KWaveSource, SimulationOutput, SourceMode, VALID_RECORD_FIELDS, db2neper,
+                   get_optimal_pml_size, get_pml, make_ball, make_circle, make_disc, make_line,
+                   make_time, neper2db, smooth, tone_burst, validate_record_fields)
+from ._lib import KWaveB200Error, LIB_PATH, load_library
+from .solver import Context, Simulation, build_problem, default_context, kspace_first_order
+
+make_time_ = make_time  # `make_time!` in the reference
+
+__all__ = [
+    "Additive", "AdditiveNoCorrection", "Dirichlet", "KWaveGrid", "KWaveMedium", "KWaveSensor",
+    "KWaveSource", "SimulationOutput", "SourceMode", "VALID_RECORD_FIELDS", "db2neper",
+    "get_optimal_pml_size", "get_pml", "make_ball", "make_circle", "make_disc", "make_line",
+    "make_time", "make_time_", "neper2db", "smooth", "tone_burst", "validate_record_fields",
+    "KWaveB200Error", "LIB_PATH", "load_library", "Context", "Simulation", "build_problem",
+    "default_context", "kspace_first_order",
+]

@@ -1,0 +1,454 @@
+"""``kspace_first_order`` on the GPU through libkwb, with the reference's signature and output.
+
+``kspace_first_order(kgrid, medium, source, sensor; ...)`` (KWave.jl/src/solver/
+first_order.jl:92-111, 287-306, 505-524) is restated as: validate and normalise the arguments
+exactly where the reference does, smooth p0 on the host in FP64 (first_order_steps.jl:70-72,
+109-111, 157-159), build one ``kwb_problem`` and call ``kwb_solve``; then apply the reference's
+post-loop host filters (first_order_steps.jl:836-910) and return a ``SimulationOutput``.
+
+Errors the reference raises are raised here with the same meaning: an unset time array, an
+invalid record field, signals with too few rows (BoundsError), ``:I_avg``/``:I_max`` with
+``data_cast=Float32`` (MethodError in ``_acoustic_intensity``), array ``alpha_coeff``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import threading
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import KWaveB200Error, check
+from .core import (KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource, SimulationOutput,
+                   SourceMode, smooth, validate_record_fields)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _ptr_d(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ptr_i(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def _flat(a, shape) -> np.ndarray:
+    """Column-major (Julia linear order) flattening of a grid-shaped array."""
+    arr = np.asarray(a, dtype=np.float64)
+    if arr.shape != tuple(shape):
+        if arr.size == int(np.prod(shape)) and arr.ndim == 1:
+            return _f64(arr)
+        raise ValueError(f"array of shape {arr.shape} does not match the grid {tuple(shape)}")
+    return _f64(arr.ravel(order="F"))
+
+
+def _findall(mask, shape) -> np.ndarray:
+    m = np.asarray(mask, dtype=bool)
+    if m.shape != tuple(shape):
+        raise ValueError(f"mask of shape {m.shape} does not match the grid {tuple(shape)}")
+    return np.ascontiguousarray(np.flatnonzero(m.ravel(order="F")).astype(np.int64))
+
+
+def _signal(sig) -> np.ndarray:
+    """A vector signal indexes as an n x 1 matrix (size(v, 2) == 1 in Julia)."""
+    s = np.asarray(sig, dtype=np.float64)
+    if s.ndim == 1:
+        s = s.reshape(-1, 1)
+    if s.ndim != 2:
+        raise ValueError("source signals must be vectors or (n_points x n_cols) matrices")
+    return np.ascontiguousarray(s.ravel(order="F")), s.shape[0], s.shape[1]
+
+
+class Context:
+    """A libkwb context bound to one CUDA device (use from one thread at a time)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load_library()
+        h = C.c_void_p()
+        rc = self.lib.kwb_context_create(device, C.byref(h))
+        if rc != _lib.KWB_OK:
+            msg = self.lib.kwb_last_error(None)
+            raise KWaveB200Error(rc, msg.decode() if msg else "context creation failed")
+        self.handle = h
+        self.device = device
+        self.lock = threading.Lock()
+
+    def close(self):
+        if self.handle:
+            self.lib.kwb_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+_default_lock = threading.Lock()
+
+
+def default_context() -> Context:
+    global _default_ctx
+    with _default_lock:
+        if _default_ctx is None:
+            _default_ctx = Context(0)
+        return _default_ctx
+
+
+class _Built:
+    """A kwb_problem plus every host array it points into (kept alive for the call)."""
+
+    def __init__(self):
+        self.keep = []
+        self.problem = _lib.Problem()
+        self.groups_py = []  # (record list, n_rows) per group
+        self.callback = None
+
+    def arr(self, a):
+        self.keep.append(a)
+        return a
+
+
+def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
+                  pml_size=20, pml_alpha=2.0, smooth_p0: bool = True, data_cast=np.float64,
+                  progress_callback=None, extra_sensors=()) -> _Built:
+    """Normalise the reference's arguments into a kwb_problem (first_order.jl:311-441, 529-669).
+
+    ``extra_sensors`` (not in the reference API) adds further sensor groups -- (mask, record)
+    pairs given as ``KWaveSensor`` or dicts -- so one solve can record different fields on
+    different masks; their outputs come back in ``SimulationOutput.extra``.
+    """
+    if kgrid.Nt == 0 or kgrid.dt == 0:
+        raise RuntimeError("Time array not set. Call make_time!(kgrid, sound_speed) before running.")
+    validate_record_fields(sensor)
+    D = kgrid.ndim
+    shape = kgrid.N
+    nvox = int(np.prod(shape))
+    b = _Built()
+    P = b.problem
+    P.ndim = D
+    for a in range(3):
+        P.N[a] = shape[a] if a < D else 1
+        P.d[a] = kgrid.d[a] if a < D else 1.0
+    P.dt = float(kgrid.dt)
+    P.Nt = int(kgrid.Nt)
+    if D == 1:
+        if isinstance(pml_size, (tuple, list)) or isinstance(pml_alpha, (tuple, list)):
+            raise TypeError("the 1D solver takes scalar pml_size and pml_alpha")
+    psz = tuple(pml_size) if isinstance(pml_size, (tuple, list)) else (pml_size,) * D
+    pal = tuple(pml_alpha) if isinstance(pml_alpha, (tuple, list)) else (pml_alpha,) * D
+    if len(psz) != D or len(pal) != D:
+        raise TypeError("pml_size / pml_alpha tuples must have one entry per dimension")
+    for a in range(D):
+        P.pml_size[a] = int(psz[a])
+        P.pml_alpha[a] = float(pal[a])
+
+    def field(v, name, optional=False):
+        f = _lib.Field()
+        if v is None:
+            if not optional:
+                raise TypeError(f"{name} is required")
+            f.count = 0
+            return f
+        arr = b.arr(_f64([float(v)]) if np.ndim(v) == 0 else _flat(v, shape))
+        f.data = _ptr_d(arr)
+        f.count = arr.size
+        return f
+
+    P.c0 = field(medium.sound_speed, "sound_speed")
+    P.rho0 = field(medium.density if medium.density is not None else 1.0, "density")
+    P.BonA = field(medium.BonA, "BonA", optional=True)
+    if medium.is_lossless():
+        P.alpha_mode = _lib.NO_ABSORPTION
+    else:
+        if np.ndim(medium.alpha_coeff) != 0:
+            raise TypeError("array alpha_coeff is not supported by the reference solver "
+                            "(T(absorb_tau) on an array, first_order.jl:369)")
+        if medium.alpha_power is None:
+            raise TypeError("alpha_power must be set when alpha_coeff is set (db2neper(x, nothing))")
+        modes = {"no_absorption": _lib.NO_ABSORPTION, "no_dispersion": _lib.NO_DISPERSION,
+                 "stokes": _lib.STOKES}
+        if medium.alpha_mode not in modes:
+            raise ValueError(f"unknown alpha_mode {medium.alpha_mode}")
+        P.alpha_mode = modes[medium.alpha_mode]
+        P.alpha_coeff = float(medium.alpha_coeff)
+        P.alpha_power = float(medium.alpha_power)
+
+    tr = sensor.is_time_reversal()
+    if source.p0 is not None and not tr:
+        p0 = np.asarray(source.p0, dtype=np.float64)
+        if p0.shape != tuple(shape):
+            raise ValueError(f"p0 of shape {p0.shape} does not match the grid {tuple(shape)}")
+        do_smooth = smooth_p0 and ((D == 1 and shape[0] > 4) or (D > 1 and all(n > 1 for n in shape)))
+        if do_smooth:
+            p0 = smooth(p0, restore_max=True)
+        arr = b.arr(_flat(p0, shape))
+        P.p0.data = _ptr_d(arr)
+        P.p0.count = nvox
+
+    if source.has_pressure_source():
+        idx = b.arr(_findall(source.p_mask, shape))
+        sig, rows, cols = _signal(source.p)
+        b.arr(sig)
+        if rows < idx.size:
+            raise IndexError(f"BoundsError: source.p has {rows} rows for {idx.size} p_mask points")
+        P.p_index = _ptr_i(idx)
+        P.n_p_index = idx.size
+        P.p_mode = int(SourceMode(source.p_mode))
+        P.p_signal.data = _ptr_d(sig)
+        P.p_signal.n_rows = rows
+        P.p_signal.n_cols = cols
+    if source.has_velocity_source():
+        idx = b.arr(_findall(source.u_mask, shape))
+        P.u_index = _ptr_i(idx)
+        P.n_u_index = idx.size
+        P.u_mode = int(SourceMode(source.u_mode))
+        for a, comp in enumerate((source.ux, source.uy, source.uz)):
+            if comp is None or a >= D:
+                continue
+            sig, rows, cols = _signal(comp)
+            b.arr(sig)
+            if rows < idx.size and idx.size > 0:
+                raise IndexError(f"BoundsError: velocity signal {a} has {rows} rows for {idx.size} u_mask points")
+            P.u_signal[a].data = _ptr_d(sig)
+            P.u_signal[a].n_rows = rows
+            P.u_signal[a].n_cols = cols
+
+    groups = []
+    sensors = [sensor] + [s if isinstance(s, KWaveSensor) else KWaveSensor(**s) for s in extra_sensors]
+    for gi, sen in enumerate(sensors):
+        if sen.mask is None:
+            if gi == 0:
+                continue
+            raise ValueError("extra sensors need a mask")
+        validate_record_fields(sen)
+        m = np.asarray(sen.mask)
+        g = _lib.SensorGroup()
+        if m.dtype == bool:
+            idx = b.arr(_findall(m, shape))
+            if idx.size == nvox and nvox > 0:
+                g.dense = 1
+                g.n_index = nvox
+            else:
+                g.index = _ptr_i(idx)
+                g.n_index = idx.size
+            n_rows = idx.size
+        else:
+            g.cartesian = 1
+            g.n_index = int(m.shape[1])
+            n_rows = int(m.shape[1])
+        rec = list(sen.record)
+        if ("I_avg" in rec or "I_max" in rec) and np.dtype(data_cast) == np.float32 and n_rows > 0 \
+                and m.dtype == bool:
+            raise TypeError("MethodError: _acoustic_intensity(::Float32, ...) -- the reference records "
+                            ":I_avg/:I_max only with data_cast=Float64")
+        for f in rec:
+            g.record_mask |= 1 << _lib.REC[f]
+            g.record_count[_lib.REC[f]] += 1
+        groups.append(g)
+        b.groups_py.append((rec, n_rows, bool(g.cartesian)))
+    if groups:
+        arr = (_lib.SensorGroup * len(groups))(*groups)
+        b.keep.append(arr)
+        P.groups = arr
+        P.n_groups = len(groups)
+
+    if tr:
+        data = np.asarray(sensor.time_reversal_boundary_data, dtype=np.float64)
+        if data.ndim == 1:
+            data = data.reshape(-1, 1)
+        flat = b.arr(np.ascontiguousarray(data.ravel(order="F")))
+        P.tr.data = _ptr_d(flat)
+        P.tr.n_rows = data.shape[0]
+        P.tr.n_cols = data.shape[1]
+
+    if progress_callback is not None:
+        def _cb(t_index, Nt, p_ptr, user):
+            p = np.ctypeslib.as_array(p_ptr, shape=(nvox,)).reshape(shape, order="F").copy()
+            progress_callback(int(t_index), int(Nt), p)
+        b.callback = _lib.PROGRESS_FN(_cb)
+        P.progress = b.callback
+    return b
+
+
+def _alloc_outputs(ctx: Context, b: _Built, kgrid: KWaveGrid):
+    lib = ctx.lib
+    ng = b.problem.n_groups
+    sizes = (_lib.GroupSizes * max(ng, 1))()
+    pf_len = C.c_int64(0)
+    check(lib, ctx.handle, lib.kwb_query_outputs(ctx.handle, C.byref(b.problem), sizes, C.byref(pf_len)))
+    outs = (_lib.GroupOutputs * max(ng, 1))()
+    arrays = []
+    for g in range(ng):
+        rec, _, _ = b.groups_py[g]
+        d = {}
+        for f in dict.fromkeys(rec):
+            i = _lib.REC[f]
+            rows, cols = sizes[g].rows[i], sizes[g].cols[i]
+            a = np.zeros(rows * cols, dtype=np.float64)
+            outs[g].field[i] = _ptr_d(a)
+            d[f] = (a, rows, cols)
+        arrays.append(d)
+    O = _lib.Outputs()
+    O.groups = outs
+    pfull = None
+    if pf_len.value > 0:
+        pfull = np.zeros(pf_len.value, dtype=np.float64)
+        O.p_final_full = _ptr_d(pfull)
+    return O, outs, arrays, pfull
+
+
+def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt_loop: int):
+    dicts = []
+    for g, d in enumerate(arrays):
+        data = {}
+        for f, (a, rows, cols) in d.items():
+            data[f] = a.reshape((rows, cols), order="F") if f in _lib.SERIES_FIELDS else a
+        dicts.append(data)
+    main = dicts[0] if (dicts and sensor.mask is not None) else {}
+    extra = dicts[1:] if sensor.mask is not None else dicts
+    if pfull is not None:
+        main["p_final"] = pfull
+    apply_sensor_directivity(main, sensor, kgrid)
+    apply_frequency_response(main, sensor, kgrid)
+    out = SimulationOutput(main)
+    out.extra = extra
+    return out
+
+
+def apply_sensor_directivity(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
+    """first_order_steps.jl:836-873 -- per-sensor sinc(k a sin(theta)/2) filter of p (host, FP64)."""
+    if sensor.directivity_angle is None or sensor.directivity_size is None or "p" not in data:
+        return
+    p = data["p"]
+    n, Nt = p.shape
+    freqs = np.fft.fftfreq(Nt, kgrid.dt)
+    dmin = kgrid.d[0] if kgrid.ndim == 1 else min(kgrid.d)
+    ang = np.asarray(sensor.directivity_angle, dtype=np.float64)
+    kval = 2 * math.pi * np.abs(freqs) / dmin
+    for j in range(n):
+        th = float(ang) if ang.ndim == 0 else float(ang.ravel()[j])
+        if abs(th) <= 1.4901161193847656e-08 * abs(th) or th == 0.0:
+            continue
+        arg = kval * sensor.directivity_size * math.sin(th) / 2
+        with np.errstate(invalid="ignore", divide="ignore"):
+            filt = np.where(arg == 0, 1.0, np.sin(arg) / np.where(arg == 0, 1.0, arg))
+        p[j, :] = np.real(np.fft.ifft(np.fft.fft(p[j, :]) * filt))
+
+
+def apply_frequency_response(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
+    """first_order_steps.jl:880-910 -- Gaussian band-pass of p (host, FP64)."""
+    if sensor.frequency_response is None or "p" not in data:
+        return
+    fc, bw = sensor.frequency_response
+    p = data["p"]
+    n, Nt = p.shape
+    resp = np.exp(-((np.abs(np.fft.fftfreq(Nt, kgrid.dt)) - fc) ** 2) / (2 * bw ** 2))
+    for j in range(n):
+        p[j, :] = np.real(np.fft.ifft(np.fft.fft(p[j, :]) * resp))
+
+
+def kspace_first_order(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
+                       sensor: KWaveSensor, *, pml_inside: bool = True, pml_size=20,
+                       pml_alpha=2.0, smooth_p0: bool = True, smooth_c0: bool = False,
+                       smooth_rho0: bool = False, data_cast=np.float64, save_to_disk=None,
+                       plot_sim: bool = False, plot_layout: str = "default", plot_scale="auto",
+                       record_movie=None, progress_callback=None, show_progress: bool = True,
+                       context: Optional[Context] = None) -> SimulationOutput:
+    """Run the fluid k-space simulation on the GPU; same arguments and output as the reference.
+
+    ``pml_inside``, ``smooth_c0``, ``smooth_rho0``, ``plot_*``, ``record_movie`` and
+    ``show_progress`` are accepted and ignored, as in the reference solver body.  Fields and
+    FFTs are FP32 whatever ``data_cast`` says; ``data_cast`` only selects the reference's error
+    behaviour for ``:I_avg``/``:I_max``.
+    """
+    if save_to_disk is not None:
+        raise NotImplementedError("save_to_disk writes an HDF5 input file for the k-Wave C++ binary; "
+                                  "HDF5 output is not part of this library")
+    ctx = context or default_context()
+    b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
+                      smooth_p0=smooth_p0, data_cast=data_cast, progress_callback=progress_callback)
+    Nt_loop = b.problem.tr.n_cols if b.problem.tr.data else b.problem.Nt
+    with ctx.lock:
+        O, outs, arrays, pfull = _alloc_outputs(ctx, b, kgrid)
+        check(ctx.lib, ctx.handle, ctx.lib.kwb_solve(ctx.handle, C.byref(b.problem), C.byref(O)))
+    if sensor.is_time_reversal():
+        kgrid.Nt = int(Nt_loop)  # the reference mutates kgrid.Nt[] (first_order.jl:430-431)
+    return _collect(b, arrays, pfull, sensor, kgrid, Nt_loop)
+
+
+class Simulation:
+    """A resident simulation: the solve split into create / advance / read (kwb_sim_*)."""
+
+    def __init__(self, kgrid, medium, source, sensor, *, pml_size=20, pml_alpha=2.0,
+                 smooth_p0=True, extra_sensors=(), context: Optional[Context] = None):
+        self.ctx = context or default_context()
+        self.kgrid, self.sensor = kgrid, sensor
+        self.b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size,
+                               pml_alpha=pml_alpha, smooth_p0=smooth_p0, extra_sensors=extra_sensors)
+        self.Nt = int(self.b.problem.tr.n_cols if self.b.problem.tr.data else self.b.problem.Nt)
+        h = C.c_void_p()
+        with self.ctx.lock:
+            check(self.ctx.lib, self.ctx.handle,
+                  self.ctx.lib.kwb_sim_create(self.ctx.handle, C.byref(self.b.problem), C.byref(h)))
+        self.handle = h
+
+    def _chk(self, rc):
+        return check(self.ctx.lib, self.ctx.handle, rc)
+
+    def advance(self, steps: int):
+        self._chk(self.ctx.lib.kwb_sim_advance(self.handle, int(steps)))
+
+    def advance_timed(self, steps: int) -> float:
+        ms = C.c_double(0)
+        self._chk(self.ctx.lib.kwb_sim_advance_timed(self.handle, int(steps), C.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        self._chk(self.ctx.lib.kwb_sim_sync(self.handle))
+
+    @property
+    def steps_done(self) -> int:
+        return int(self.ctx.lib.kwb_sim_steps_done(self.handle))
+
+    def pressure(self) -> np.ndarray:
+        n = int(np.prod(self.kgrid.N))
+        out = np.empty(n, dtype=np.float32)
+        self._chk(self.ctx.lib.kwb_sim_read_pressure(self.handle, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out.reshape(self.kgrid.N, order="F")
+
+    def outputs(self) -> SimulationOutput:
+        O, outs, arrays, pfull = _alloc_outputs(self.ctx, self.b, self.kgrid)
+        self._chk(self.ctx.lib.kwb_sim_read_outputs(self.handle, C.byref(O)))
+        return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt)
+
+    def profile(self, steps: int) -> list:
+        kt = _lib.KernelTimes()
+        self._chk(self.ctx.lib.kwb_sim_profile(self.handle, int(steps), C.byref(kt)))
+        return [dict(name=kt.name[i].value.decode(), total_ms=kt.total_ms[i], launches=kt.launches[i],
+                     bytes_per_launch=kt.bytes_per_launch[i]) for i in range(kt.n)]
+
+    def info(self):
+        nb = C.c_int64(0)
+        nl = C.c_int32(0)
+        self._chk(self.ctx.lib.kwb_sim_info(self.handle, C.byref(nb), C.byref(nl)))
+        return {"device_bytes": nb.value, "launches_per_step": nl.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.ctx.lib.kwb_sim_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
