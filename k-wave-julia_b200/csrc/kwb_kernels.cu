@@ -576,9 +576,18 @@ size_t spec_pass_smem(int N, int L, int dispersion) {
 
 static int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// The dynamic shared-memory limit of a kernel is a per-function attribute.  It is raised once to
+// the device's opt-in maximum, so simulations of different sizes in one process never lower
+// it under one another.
 static cudaError_t set_smem(const void *fn, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (bytes > (size_t)optin) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
 }
 
 cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
