@@ -193,6 +193,33 @@ int kwb_sim_profile(kwb_sim *sim, int64_t steps, kwb_kernel_times *out);
 /* Device bytes the simulation holds and kernels launched per time step. */
 int kwb_sim_info(const kwb_sim *sim, int64_t *device_bytes, int32_t *launches_per_step);
 
+/* ---- equation of state without device allocation ----------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc -- hosts that own
+ * all device memory through their own pool and forbid hidden allocations, real-time loops that
+ * must not allocate after start-up -- this computes one equation-of-state step,
+ *   p = irfftn( M .* rfftn( [c0^2] rho_eff ) ),  rho_eff = rho (1 + Q rho),  rho = sum_d rho_d,
+ *   M = [c0^2] kappa (1 + tau |k|^y) / (Nx Ny Nz)          (first_order_steps.jl:214-290 without
+ *                                                           the :stokes dispersion branch)
+ * with the same kernels as kwb_solve, from caller-owned device arrays (FP32, column-major):
+ * rho[0..ndim-1], optional c0sq (c0^2 per voxel; NULL = scalar c0sq_scalar), optional nlq
+ * (Q = BonA/(2 rho0) per voxel; NULL = nlq_scalar, used when nonlinear != 0), output p.
+ * Its scratch (descriptor, twiddles, multiplier, half spectrum) is one static device array of
+ * KWB_NOALLOC_SCRATCH_MIB MiB that every GPU loading libkwb holds until exit.  Limits: the half
+ * spectrum (Nx/2+1)*Ny*Nz must not exceed KWB_NOALLOC_MAX_SPECTRUM (else KWB_E_UNSUPPORTED);
+ * alpha_mode KWB_STOKES with scalar c0 (the dispersion branch) is rejected.  The work is queued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream) and the call returns without waiting.
+ * The first call on a device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the array: calls whose GPU work overlaps race on it and
+ * must be serialised by the caller.  Errors: kwb_noalloc_last_error(). */
+#define KWB_NOALLOC_SCRATCH_MIB 32
+#define KWB_NOALLOC_MAX_SPECTRUM 2621440
+int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t N[3], const double d[3],
+                             double dt, double c_ref, int32_t alpha_mode, double alpha_coeff,
+                             double alpha_power, const float *const rho[3], const float *c0sq,
+                             float c0sq_scalar, const float *nlq, float nlq_scalar,
+                             int32_t nonlinear, float *p, void *stream);
+const char *kwb_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
