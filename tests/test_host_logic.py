@@ -1,0 +1,108 @@
+"""CPU checks of the host-side mirror: setup helpers agree with the oracle's restatement, and
+build_problem turns the reference's arguments into the kwb_problem the C ABI expects."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import kwave_b200 as kb
+import kwave_ref as K
+from kwave_b200 import workloads as W
+
+
+def test_setup_helpers_match_oracle():
+    rng = np.random.default_rng(5)
+    for shape in [(32,), (16, 12), (9, 8, 7)]:
+        m = rng.standard_normal(shape)
+        assert np.allclose(kb.smooth(m, restore_max=True), K.smooth(m, restore_max=True), atol=1e-12)
+    for args in [(40e6, 1e6, 5), (1 / 2e-8, 1e6, 5), (1 / 3.6e-8, 1.3e6, 3)]:
+        for env in ("gaussian", "rectangular", "cosine"):
+            assert np.array_equal(kb.tone_burst(*args, envelope=env), K.tone_burst(*args, envelope=env)) or \
+                np.allclose(kb.tone_burst(*args, envelope=env), K.tone_burst(*args, envelope=env), atol=1e-15)
+    assert np.array_equal(kb.make_disc(64, 48, 20, 30, 7), K.make_disc(64, 48, 20, 30, 7))
+    assert np.array_equal(kb.make_circle(64, 48, 20, 30, 11), K.make_circle(64, 48, 20, 30, 11))
+    assert np.array_equal(kb.make_line(20, 30, (2, 3), (19, 27)), K.make_line(20, 30, (2, 3), (19, 27)))
+    assert np.array_equal(kb.make_ball(20, 18, 16, 9, 8, 7, 5), K.make_ball(20, 18, 16, 9, 8, 7, 5))
+    for st in (False, True):
+        assert np.array_equal(kb.get_pml(50, 1e-4, 12, 2.0, 2e-8, st), K.get_pml(50, 1e-4, 12, 2.0, 2e-8, st))
+    assert kb.get_optimal_pml_size((100, 128, 77)) == K.get_optimal_pml_size((100, 128, 77))
+    assert kb.db2neper(0.75, 1.5) == K.db2neper(0.75, 1.5)
+    g1, g2 = kb.KWaveGrid(128, 1e-4, 96, 2e-4), K.KWaveGrid(128, 1e-4, 96, 2e-4)
+    assert kb.make_time(g1, 1500.0) == K.make_time(g2, 1500.0)
+    for a in range(2):
+        assert np.array_equal(g1.k_vec(a), g2.k_vecs[a])
+
+
+def test_build_problem_layout():
+    n0, n1 = 12, 10
+    g = kb.KWaveGrid(n0, 1e-4, n1, 2e-4)
+    kb.make_time(g, 1500.0, t_end=1e-6)
+    c = np.arange(n0 * n1, dtype=float).reshape(n0, n1) + 1400
+    pm = np.zeros((n0, n1), bool)
+    pm[3, 2] = pm[1, 5] = pm[7, 2] = True
+    sig = np.arange(6.0).reshape(3, 2)
+    sm = np.zeros((n0, n1), bool)
+    sm[0, 0] = sm[11, 9] = True
+    b = kb.build_problem(g, kb.KWaveMedium(sound_speed=c, density=1000.0, alpha_coeff=0.5, alpha_power=1.2,
+                                           alpha_mode="stokes", BonA=5.0),
+                         kb.KWaveSource(p_mask=pm, p=sig, p_mode=kb.Dirichlet),
+                         kb.KWaveSensor(mask=sm, record=["p", "p_rms", "p_rms"]), pml_size=(4, 6), pml_alpha=(2.0, 3.0))
+    P = b.problem
+    assert P.ndim == 2 and list(P.N) == [n0, n1, 1] and P.Nt == g.Nt
+    assert list(P.pml_size)[:2] == [4, 6] and list(P.pml_alpha)[:2] == [2.0, 3.0]
+    # column-major (x fastest) linear indices, sorted, as findall returns
+    idx = [P.p_index[i] for i in range(P.n_p_index)]
+    assert idx == sorted([3 + n0 * 2, 7 + n0 * 2, 1 + n0 * 5])
+    assert P.c0.count == n0 * n1 and P.c0.data[3 + n0 * 2] == c[3, 2]
+    assert P.p_signal.n_rows == 3 and P.p_signal.n_cols == 2 and P.p_signal.data[1] == sig[1, 0]
+    assert P.p_mode == 0 and P.alpha_mode == 2 and P.BonA.count == 1
+    grp = P.groups[0]
+    assert grp.n_index == 2 and grp.dense == 0 and [grp.index[0], grp.index[1]] == [0, n0 * n1 - 1]
+    assert grp.record_mask == (1 << 0) | (1 << 3) and grp.record_count[3] == 2
+
+
+def test_build_problem_dense_cartesian_tr_and_errors():
+    g = kb.KWaveGrid(8, 1e-4, 8, 1e-4)
+    med = kb.KWaveMedium(sound_speed=1500.0)
+    with pytest.raises(RuntimeError, match="make_time"):
+        kb.build_problem(g, med, kb.KWaveSource(), kb.KWaveSensor())
+    kb.make_time(g, 1500.0, t_end=1e-7)
+    b = kb.build_problem(g, med, kb.KWaveSource(), kb.KWaveSensor(mask=np.ones((8, 8), bool), record=["p_max"]))
+    assert b.problem.groups[0].dense == 1 and b.problem.groups[0].n_index == 64
+    b = kb.build_problem(g, med, kb.KWaveSource(), kb.KWaveSensor(mask=np.zeros((2, 7)), record=["p"]))
+    assert b.problem.groups[0].cartesian == 1 and b.problem.groups[0].n_index == 7
+    tr = np.ones((4, 9))
+    m = np.zeros((8, 8), bool)
+    m[0, :4] = True
+    b = kb.build_problem(g, med, kb.KWaveSource(p0=np.ones((8, 8))),
+                         kb.KWaveSensor(mask=m, time_reversal_boundary_data=tr, record=["p_final"]))
+    assert b.problem.tr.n_rows == 4 and b.problem.tr.n_cols == 9 and b.problem.p0.count == 0
+    with pytest.raises(ValueError, match="Invalid sensor record field"):
+        kb.build_problem(g, med, kb.KWaveSource(), kb.KWaveSensor(mask=m, record=["bogus"]))
+    with pytest.raises(TypeError, match="array alpha_coeff"):
+        kb.build_problem(g, kb.KWaveMedium(sound_speed=1500.0, alpha_coeff=np.ones((8, 8)), alpha_power=1.5,
+                                           alpha_mode="no_dispersion"), kb.KWaveSource(), kb.KWaveSensor())
+    with pytest.raises(IndexError, match="BoundsError"):
+        kb.build_problem(g, med, kb.KWaveSource(p_mask=m, p=np.ones((2, 3))), kb.KWaveSensor())
+    with pytest.raises(TypeError, match="MethodError"):
+        kb.build_problem(g, med, kb.KWaveSource(), kb.KWaveSensor(mask=m, record=["I_max"]), data_cast=np.float32)
+    with pytest.raises(NotImplementedError):
+        kb.kspace_first_order(g, med, kb.KWaveSource(), kb.KWaveSensor(), save_to_disk="/tmp/x.h5")
+
+
+def test_workloads_are_seeded_and_match_their_configs():
+    a, b = W.c2(n=64, Nt=10), W.c2(n=64, Nt=10)
+    assert np.array_equal(a.medium["sound_speed"], b.medium["sound_speed"])
+    c2 = W.c2(n=512, Nt=2000)
+    c = c2.medium["sound_speed"]
+    assert c.min() == pytest.approx(1400) and c.max() == pytest.approx(1600)
+    assert c2.dt == pytest.approx(0.3e-4 / 1600) and c2.Nt == 2000
+    c1 = W.c1()
+    assert c1.Nt == 689 and c1.source["p_mask"].sum() == 81 and c1.sensor["mask"].sum() == 228
+    assert c1.source["p"].shape == (81, 689)
+    c3 = W.c3(n=64, Nt=20, piston=8, pml=4)
+    assert c3.source["u_mask"].sum() == 64 and set(np.unique(c3.medium["BonA"])) == {5.0, 9.0}
+    sides = {W.c4_sim(i).N for i in range(8)}
+    assert all(n in W.C4_SIDES for s in sides for n in s)
+    assert W.smooth_sides(256, 300) == [256, 270, 288, 300]
