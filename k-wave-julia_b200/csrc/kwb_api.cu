@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -452,6 +453,15 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
                         std::pow(2.0 * kPi * 1e6, -y);
     tau = -2.0 * a_np * std::pow(c_ref, y - 1.0);
     eta = 2.0 * a_np * std::pow(c_ref, y - 1.0) * std::tan(kPi * y / 2.0);
+  }
+
+  // ---- FFT path: register-FFT kernels for power-of-two lines unless KWB_FFT_PATH=generic
+  {
+    const char *fp = getenv("KWB_FFT_PATH");
+    h.fast = 3;  // bit 0: line passes, bit 1: equation-of-state passes
+    if (fp && strcmp(fp, "generic") == 0) h.fast = 0;
+    if (fp && strcmp(fp, "line") == 0) h.fast = 1;
+    if (fp && strcmp(fp, "eos") == 0) h.fast = 2;
   }
 
   // ---- tile shapes and FFT plans

@@ -100,6 +100,8 @@ struct SimDev {
 
   long long Nt;
   const long long *t0;  // device step base (CUDA graph replays advance it)
+
+  int fast;  // register-FFT kernels (kwb_fast.cu) for power-of-two lines: bit 0 line passes, bit 1 EOS passes
 };
 
 // Sensor group on the device.
@@ -136,6 +138,15 @@ cudaError_t launch_sensor_gather(const SimDev *d_sim, const SimDev &h, const Gro
 cudaError_t launch_advance_t0(long long *t0, long long k, cudaStream_t st);
 // Raise the dynamic shared-memory limit of every time-step kernel for this simulation's tiles.
 cudaError_t prime_attributes(const SimDev &h);
+
+// Register-FFT kernels (kwb_fast.cu) for line lengths 64, 128, 256, 512, 1024.
+bool fast_size(int N);
+cudaError_t fast_prime(int N);
+cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                           cudaStream_t st);
+cudaError_t fast_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
+cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                      cudaStream_t st);
 
 // FP64 table builders.
 cudaError_t build_twiddles(float2 *out, int N, cudaStream_t st);

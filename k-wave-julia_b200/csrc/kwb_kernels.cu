@@ -592,6 +592,7 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
 
 cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
                              long long step_s, cudaStream_t st) {
+  if ((h.fast & 1) && fast_size(h.N[axis])) return fast_line_pass(d_sim, h, axis, mode, step_s, st);
   const int L = h.L_line[axis];
   const size_t sm = line_pass_smem(h.N[axis], L);
   int tiles;
@@ -607,6 +608,7 @@ cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int
 
 cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long step_s,
                              cudaStream_t st) {
+  if ((h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0])) return fast_eos(d_sim, h, true, step_s, st);
   const int L = h.L_eosx;
   const size_t sm = spec_pass_smem(h.N[0], L, h.dispersion);
   const int tiles = cdiv(h.N[1], 2 * L) * h.N[2];
@@ -616,6 +618,7 @@ cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long ste
 
 cudaError_t launch_eos_x_inv(const SimDev *d_sim, const SimDev &h, long long step_s,
                              cudaStream_t st) {
+  if ((h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0])) return fast_eos(d_sim, h, false, step_s, st);
   const int L = h.L_eosx;
   const size_t sm = line_pass_smem(h.N[0], L);
   const int tiles = cdiv(h.N[1], 2 * L) * h.N[2];
@@ -625,6 +628,7 @@ cudaError_t launch_eos_x_inv(const SimDev *d_sim, const SimDev &h, long long ste
 
 cudaError_t launch_spec_pass(const SimDev *d_sim, const SimDev &h, int axis, int op,
                              long long step_s, cudaStream_t st) {
+  if ((h.fast & 2) && !h.dispersion && fast_size(h.N[axis])) return fast_spec(d_sim, h, axis, op, step_s, st);
   const int L = h.L_spec[axis];
   const size_t sm = spec_pass_smem(h.N[axis], L, h.dispersion && op != KWB_SPEC_INV);
   const int tiles = cdiv(h.n1, L) * (axis == 1 ? h.N[2] : h.N[1]);
@@ -657,7 +661,11 @@ cudaError_t prime_attributes(const SimDev &h) {
   if ((e = set_smem((const void *)k_eos_x_inv, line_pass_smem(h.N[0], h.L_eosx))) != cudaSuccess) return e;
   m = 0;
   for (int a = 1; a < h.ndim; ++a) m = std::max(m, spec_pass_smem(h.N[a], h.L_spec[a], h.dispersion));
-  return set_smem((const void *)k_spec_pass, m);
+  if ((e = set_smem((const void *)k_spec_pass, m)) != cudaSuccess) return e;
+  if (h.fast)
+    for (int a = 0; a < h.ndim; ++a)
+      if (fast_size(h.N[a]) && (e = fast_prime(h.N[a])) != cudaSuccess) return e;
+  return cudaSuccess;
 }
 
 cudaError_t launch_advance_t0(long long *t0, long long k, cudaStream_t st) {
