@@ -11,6 +11,8 @@
 //
 // Same semantics as the generic shared-memory Stockham kernels (kwb_kernels.cu), which keep
 // serving every other line length (radix 3/5/7 sizes) and the :stokes dispersion branch.
+#include <algorithm>
+
 #include "kwb_fft.cuh"
 
 namespace kwb {
@@ -148,19 +150,39 @@ __device__ __forceinline__ void build_tables(float2 *tw2, float2 *gp2, float2 *g
 }
 
 template <int E, int G>
-constexpr size_t line_smem(int L) {
+__host__ __device__ constexpr size_t line_smem(int L) {
   return ((size_t)L * (E * (G + 1) + 1) + 3 * (size_t)E * (G + 1)) * sizeof(float2);
 }
+// Line pass: the exchange buffers and tables, then two staged operand tiles (p and rho0) of
+// 2L real lines x N floats each, 16-byte aligned.
+template <int E, int G>
+__host__ __device__ constexpr size_t line_stage_offset(int L) {
+  return (line_smem<E, G>(L) + 15) & ~size_t(15);
+}
+template <int E, int G>
+__host__ __device__ constexpr size_t line_smem_staged(int L) {
+  return line_stage_offset<E, G>(L) + 2 * (size_t)(2 * L) * (E * G) * sizeof(float);
+}
+
+// 16-byte asynchronous global->shared copy; bytes beyond src_bytes are zero-filled.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // ------------------------------------------------------------------------------------------
 // fused per-axis line pass (same algorithm as kwb::k_line_pass)
 // ------------------------------------------------------------------------------------------
 
-template <int E, int G, bool CONTIG>
-__global__ void __launch_bounds__(KWB_THREADS)
+template <int E, int G, bool CONTIG, int LT>
+__global__ void __launch_bounds__(LT * G, E <= 16 ? 2 * (KWB_THREADS / (LT * G)) : 1)
     k_line_fast(const SimDev *__restrict__ sims, int axis, int mode, long long step_s) {
   using F = LineFFT<E, G, CONTIG>;
-  constexpr int L = KWB_THREADS / G, RP = F::RP, LP = F::LP;
+  constexpr int RP = F::RP, LP = F::LP;
+  constexpr int L = LT;  // complex lines per tile
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
@@ -200,31 +222,58 @@ __global__ void __launch_bounds__(KWB_THREADS)
     first_line = x0 + Nx * o;
   }
   const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
-  const bool pair = !CONTIG && vb && ((stride & 1) == 0) && ((base & 1) == 0);
-  auto addr = [&](int c, int i) -> long long {
-    return CONTIG ? base + (long long)c * Nx + i : base + (long long)i * stride + c;
-  };
+  // Element (column c, position i) sits at off(c, i) from `base`; 32-bit offsets (grids are
+  // limited to 2^31 voxels).  Strided tiles read the two columns of a pair as one float2 (the
+  // row pitch is even on this path), zero-filling a pair that lies past the grid edge.
+  const int st32 = (int)stride;
+  auto off = [&](int c, int i) -> int { return CONTIG ? c * Nx + i : i * st32 + c; };
   auto load_pair = [&](const float *__restrict__ f, int i) -> float2 {
-    if (pair) return __ldg(reinterpret_cast<const float2 *>(f + addr(2 * l, i)));
-    return make_float2(va ? __ldg(f + addr(2 * l, i)) : 0.f, vb ? __ldg(f + addr(2 * l + 1, i)) : 0.f);
+    const float *fb = f + base;
+    if (!CONTIG) return vb ? __ldg(reinterpret_cast<const float2 *>(fb + off(2 * l, i))) : make_float2(0.f, 0.f);
+    return make_float2(va ? __ldg(fb + off(2 * l, i)) : 0.f, vb ? __ldg(fb + off(2 * l + 1, i)) : 0.f);
   };
   auto store_pair = [&](float *f, int i, float2 v) {
-    if (pair) {
-      *reinterpret_cast<float2 *>(f + addr(2 * l, i)) = v;
+    float *fb = f + base;
+    if (!CONTIG) {
+      if (vb) *reinterpret_cast<float2 *>(fb + off(2 * l, i)) = v;
       return;
     }
-    if (va) f[addr(2 * l, i)] = v.x;
-    if (vb) f[addr(2 * l + 1, i)] = v.y;
+    if (va) fb[off(2 * l, i)] = v.x;
+    if (vb) fb[off(2 * l + 1, i)] = v.y;
   };
 
+  // Stage the p tile (and the rho0 tile when density varies) into shared memory with
+  // asynchronous 16-byte copies: every load of the tile is in flight at once, overlapping the
+  // table set-up and, for rho0, the first transform.  Staged layout: CONTIG [row][i],
+  // strided [i][column] (the tile's own global layout, compacted).
+  float *st_p = reinterpret_cast<float *>(reinterpret_cast<char *>(smem_raw) + line_stage_offset<E, G>(L));
+  float *st_r = st_p + 2 * L * N;
+  auto stage = [&](float *dst, const float *f) {
+    const float *fb = f + base;
+    if (CONTIG) {
+      const int chunks = cnt * N / 4;  // the tile's rows are contiguous in memory
+      for (int q = tid; q < chunks; q += blockDim.x) cp_async16(dst + 4 * q, fb + 4 * q, 16);
+    } else {
+      constexpr int CPR = (2 * L) / 4;  // 16-byte chunks per tile row (strided tiles have L >= 2)
+      for (int q = tid; q < CPR * N; q += blockDim.x) {
+        const int i = q / CPR, ch = q - i * CPR;
+        const int valid = min(4, cnt - 4 * ch);
+        cp_async16(dst + i * 2 * L + 4 * ch, fb + (long long)i * st32 + 4 * ch, valid > 0 ? 4 * valid : 0);
+      }
+    }
+    cp_async_commit();
+  };
+  auto staged = [&](const float *st, int i) -> float2 {
+    if (CONTIG) return make_float2(va ? st[(2 * l) * N + i] : 0.f, vb ? st[(2 * l + 1) * N + i] : 0.f);
+    return *reinterpret_cast<const float2 *>(st + i * 2 * L + 2 * l);
+  };
+  const float *__restrict__ rho0 = S.rho0;
+  stage(st_p, S.p);
+  if (rho0) stage(st_r, rho0);
+  else cp_async_commit();
   build_tables<E, G>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
   float2 *xs = sm + l * LP;
-
-  float2 v[E];
-#pragma unroll
-  for (int r = 0; r < E; ++r) v[r] = load_pair(S.p, tt + G * r);
   float *__restrict__ ud = S.u[axis];
-  const float *__restrict__ rho0 = S.rho0;
   // operand prefetch ahead of the transform arithmetic (dropped for E = 32 to stay in registers)
   constexpr bool PF = E <= 16;
   float2 uu[PF ? E : 1];
@@ -232,13 +281,19 @@ __global__ void __launch_bounds__(KWB_THREADS)
 #pragma unroll
     for (int r = 0; r < E; ++r) uu[PF ? r : 0] = load_pair(ud, tt + G * r);
   }
-  __syncthreads();  // tables
+  cp_async_wait<1>();  // the p tile has landed (rho0 may still be in flight)
+  __syncthreads();     // ... for every thread; tables too
+  float2 v[E];
+#pragma unroll
+  for (int r = 0; r < E; ++r) v[r] = staged(st_p, tt + G * r);
 
   // d/dx_d p  (staggered +)
   F::fwd(v, xs, tw2, tt);
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gp2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
+  cp_async_wait<0>();
+  __syncthreads();  // the rho0 tile has landed
 
   // velocity update u = pml_sg (pml_sg u - dt/rho_sg dp)
   const float *__restrict__ esg = S.pml_sg_def[axis];
@@ -248,7 +303,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
     const int inext = (i + 1 == N) ? 0 : i + 1;
     float2 coef;
     if (rho0) {
-      const float2 r0 = load_pair(rho0, i), r1 = load_pair(rho0, inext);
+      const float2 r0 = staged(st_r, i), r1 = staged(st_r, inext);
       coef = make_float2(S.dt / (0.5f * (r0.x + r1.x)), S.dt / (0.5f * (r0.y + r1.y)));
     } else {
       coef = make_float2(S.dt_over_rho0_s, S.dt_over_rho0_s);
@@ -274,7 +329,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
     for (int r = 0; r < E; ++r) {
       const int i = tt + G * r;
       store_pair(ud, i, v[r]);
-      const float2 pp = load_pair(S.p, i);
+      const float2 pp = staged(st_p, i);
       float2 cs = S.c0sq ? load_pair(S.c0sq, i) : make_float2(S.c0sq_s, S.c0sq_s);
       store_pair(rd, i, make_float2(pp.x / ((float)S.D * cs.x), pp.y / ((float)S.D * cs.y)));
     }
@@ -322,7 +377,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
     const float ei = __ldg(ed + i);
     float2 coef;
     if (rho0) {
-      const float2 r0 = load_pair(rho0, i);
+      const float2 r0 = staged(st_r, i);
       coef = make_float2(S.dt * r0.x, S.dt * r0.y);
     } else {
       coef = make_float2(S.dt_rho0_s, S.dt_rho0_s);
@@ -359,11 +414,11 @@ __global__ void __launch_bounds__(KWB_THREADS)
 // equation of state: x R2C, y/z C2C with the multiply innermost, x C2R
 // ------------------------------------------------------------------------------------------
 
-template <int E, int G>
-__global__ void __launch_bounds__(KWB_THREADS)
+template <int E, int G, int LT>
+__global__ void __launch_bounds__(LT * G)
     k_eos_fwd_fast(const SimDev *__restrict__ sims, long long step_s) {
   using F = LineFFT<E, G, true>;
-  constexpr int L = KWB_THREADS / G, LP = F::LP, N = E * G;
+  constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
@@ -378,22 +433,42 @@ __global__ void __launch_bounds__(KWB_THREADS)
   const long long base = ((long long)z * Ny + y0) * N;
   const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
   build_tables<E, G>(tw2, nullptr, nullptr, S.tw[0], nullptr, nullptr);
+  // One field at a time over all E positions: each loop issues 2E independent loads, so
+  // every thread keeps many requests in flight (the sum, nonlinearity and c^2 follow).
+  auto ld = [&](const float *__restrict__ f, int i) -> float2 {
+    const float *fb = f + base + (long long)(2 * l) * N + i;
+    return make_float2(va ? __ldg(fb) : 0.f, vb ? __ldg(fb + N) : 0.f);
+  };
   float2 v[E];
 #pragma unroll
-  for (int r = 0; r < E; ++r) {
-    const int i = tt + G * r;
-    float f[2] = {0.f, 0.f};
+  for (int r = 0; r < E; ++r) v[r] = ld(S.rho[0], tt + G * r);
+  if (S.D > 1) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (!(h ? vb : va)) continue;
-      const long long a = base + (long long)(2 * l + h) * N + i;
-      float rho = __ldg(S.rho[0] + a);
-      if (S.D > 1) rho += __ldg(S.rho[1] + a);
-      if (S.D > 2) rho += __ldg(S.rho[2] + a);
-      if (S.nonlinear) rho = rho * fmaf(S.nlq ? __ldg(S.nlq + a) : S.nlq_s, rho, 1.0f);
-      f[h] = S.c0sq ? __ldg(S.c0sq + a) * rho : rho;
+    for (int r = 0; r < E; ++r) {
+      const float2 b = ld(S.rho[1], tt + G * r);
+      v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
     }
-    v[r] = make_float2(f[0], f[1]);
+  }
+  if (S.D > 2) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const float2 b = ld(S.rho[2], tt + G * r);
+      v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+    }
+  }
+  if (S.nonlinear) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const float2 q = S.nlq ? ld(S.nlq, tt + G * r) : make_float2(S.nlq_s, S.nlq_s);
+      v[r] = make_float2(v[r].x * fmaf(q.x, v[r].x, 1.0f), v[r].y * fmaf(q.y, v[r].y, 1.0f));
+    }
+  }
+  if (S.c0sq) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const float2 c = ld(S.c0sq, tt + G * r);
+      v[r] = make_float2(c.x * v[r].x, c.y * v[r].y);
+    }
   }
   __syncthreads();
   float2 *xs = sm + l * LP;
@@ -411,11 +486,11 @@ __global__ void __launch_bounds__(KWB_THREADS)
   }
 }
 
-template <int E, int G>
-__global__ void __launch_bounds__(KWB_THREADS)
+template <int E, int G, int LT>
+__global__ void __launch_bounds__(LT * G)
     k_eos_inv_fast(const SimDev *__restrict__ sims, long long step_s) {
   using F = LineFFT<E, G, true>;
-  constexpr int L = KWB_THREADS / G, LP = F::LP, N = E * G;
+  constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
@@ -447,22 +522,63 @@ __global__ void __launch_bounds__(KWB_THREADS)
   float2 v[E];
 #pragma unroll
   for (int idx = 0; idx < E; ++idx) v[idx] = xs[F::k_of(tt, idx)];
+  // dense pressure sensor (record_sensor_data!, first_order_steps.jl:732-752): prefetch the
+  // running max/min before the transform, update all fields as p is written
+  const GroupDev *gd = S.dense_p;
+  const unsigned gm = gd ? gd->mask : 0u;
+  constexpr bool PFS = E <= 16;  // prefetch only while it fits in registers
+  float2 pm[PFS ? E : 1], pn[PFS ? E : 1];
+  const long long ra = base + (long long)(2 * l) * N, rb = ra + N;
+  if (PFS && (gm & (1u << 1))) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int i = tt + G * r;
+      pm[PFS ? r : 0] = make_float2(va ? gd->pmax[ra + i] : 0.f, vb ? gd->pmax[rb + i] : 0.f);
+    }
+  }
+  if (PFS && (gm & (1u << 2))) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int i = tt + G * r;
+      pn[PFS ? r : 0] = make_float2(va ? gd->pmin[ra + i] : 0.f, vb ? gd->pmin[rb + i] : 0.f);
+    }
+  }
   __syncwarp();
   F::inv(v, xs, tw2, tt);
   float *__restrict__ p = S.p;
 #pragma unroll
   for (int r = 0; r < E; ++r) {
     const int i = tt + G * r;
-    if (va) p[base + (long long)(2 * l) * N + i] = v[r].x;
-    if (vb) p[base + (long long)(2 * l + 1) * N + i] = v[r].y;
+    if (va) p[ra + i] = v[r].x;
+    if (vb) p[rb + i] = v[r].y;
+  }
+  if (gm) {
+    const bool last = (t == S.Nt - 1);
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int i = tt + G * r;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (!(h ? vb : va)) continue;
+        const long long vx = (h ? rb : ra) + i;
+        const float pv = h ? v[r].y : v[r].x;
+        if (gm & (1u << 0)) gd->ser_p[t * gd->n + vx] = pv;
+        if (gm & (1u << 1))
+          gd->pmax[vx] = fmaxf(PFS ? (h ? pm[PFS ? r : 0].y : pm[PFS ? r : 0].x) : gd->pmax[vx], pv);
+        if (gm & (1u << 2))
+          gd->pmin[vx] = fminf(PFS ? (h ? pn[PFS ? r : 0].y : pn[PFS ? r : 0].x) : gd->pmin[vx], pv);
+        if (gm & (1u << 3)) gd->prms[vx] += (double)gd->cnt_prms * ((double)pv * (double)pv);
+        if ((gm & (1u << 4)) && last) gd->pfinal[vx] = pv;
+      }
+    }
   }
 }
 
-template <int E, int G>
-__global__ void __launch_bounds__(KWB_THREADS)
+template <int E, int G, int LT>
+__global__ void __launch_bounds__(LT * G)
     k_spec_fast(const SimDev *__restrict__ sims, int axis, int op, long long step_s) {
   using F = LineFFT<E, G, false>;
-  constexpr int L = KWB_THREADS / G, LP = F::LP;
+  constexpr int LP = F::LP, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
@@ -540,48 +656,83 @@ static cudaError_t raise_smem(const void *fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
 }
 
+// Two compile-time tile sizes per line length: full tiles of 256/G complex lines for large
+// grids, and small tiles (one warp, >= 2 lines) when full tiles would leave SMs idle.
+template <int G>
+struct Tiles {
+  static constexpr int BIG = KWB_THREADS / G;
+  static constexpr int SMALL = (32 / G > 2 ? 32 / G : 2);
+};
+
+template <int E, int G, int LT>
+static cudaError_t prime_lt() {
+  cudaError_t e;
+  const size_t ln = line_smem<E, G>(LT), lst = line_smem_staged<E, G>(LT);
+  if ((e = raise_smem((const void *)k_line_fast<E, G, true, LT>, lst)) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_line_fast<E, G, false, LT>, lst)) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_fwd_fast<E, G, LT>, ln)) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_inv_fast<E, G, LT>, ln)) != cudaSuccess) return e;
+  return raise_smem((const void *)k_spec_fast<E, G, LT>, ln);
+}
+
 template <int E, int G>
 static cudaError_t prime_size() {
-  cudaError_t e;
-  const size_t ln = line_smem<E, G>(KWB_THREADS / G);
-  if ((e = raise_smem((const void *)k_line_fast<E, G, true>, ln)) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_line_fast<E, G, false>, ln)) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_eos_fwd_fast<E, G>, ln)) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_eos_inv_fast<E, G>, ln)) != cudaSuccess) return e;
-  return raise_smem((const void *)k_spec_fast<E, G>, ln);
+  cudaError_t e = prime_lt<E, G, Tiles<G>::BIG>();
+  if (e != cudaSuccess) return e;
+  return prime_lt<E, G, Tiles<G>::SMALL>();
+}
+
+static bool want_small(const SimDev &h, long long tiles_big) {
+  return tiles_big < 2LL * (h.num_sms > 0 ? h.num_sms : 148);
+}
+
+template <int E, int G, int LT>
+static void line_go(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s, cudaStream_t st) {
+  if (axis == 0)
+    k_line_fast<E, G, true, LT><<<cdiv(h.N[1], 2 * LT) * h.N[2], LT * G, line_smem_staged<E, G>(LT), st>>>(d_sim, axis, mode, s);
+  else
+    k_line_fast<E, G, false, LT><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * G,
+                                   line_smem_staged<E, G>(LT), st>>>(d_sim, axis, mode, s);
 }
 
 template <int E, int G>
 static cudaError_t launch_line(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
                                cudaStream_t st) {
-  constexpr int L = KWB_THREADS / G;
-  const size_t sm = line_smem<E, G>(L);
-  if (axis == 0) {
-    k_line_fast<E, G, true><<<cdiv(h.N[1], 2 * L) * h.N[2], KWB_THREADS, sm, st>>>(d_sim, axis, mode, s);
-  } else {
-    const int outer = axis == 1 ? h.N[2] : h.N[1];
-    k_line_fast<E, G, false><<<cdiv(h.N[0], 2 * L) * outer, KWB_THREADS, sm, st>>>(d_sim, axis, mode, s);
-  }
+  constexpr int B = Tiles<G>::BIG;
+  const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * B) * h.N[2]
+                                    : (long long)cdiv(h.N[0], 2 * B) * (axis == 1 ? h.N[2] : h.N[1]);
+  if (want_small(h, tiles)) line_go<E, G, Tiles<G>::SMALL>(d_sim, h, axis, mode, s, st);
+  else line_go<E, G, B>(d_sim, h, axis, mode, s, st);
   return cudaGetLastError();
+}
+
+template <int E, int G, int LT>
+static void eos_go(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
+  const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
+  if (fwd) k_eos_fwd_fast<E, G, LT><<<grid, LT * G, line_smem<E, G>(LT), st>>>(d_sim, s);
+  else k_eos_inv_fast<E, G, LT><<<grid, LT * G, line_smem<E, G>(LT), st>>>(d_sim, s);
 }
 
 template <int E, int G>
 static cudaError_t launch_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
-  constexpr int L = KWB_THREADS / G;
-  const size_t sm = line_smem<E, G>(L);
-  const int grid = cdiv(h.N[1], 2 * L) * h.N[2];
-  if (fwd) k_eos_fwd_fast<E, G><<<grid, KWB_THREADS, sm, st>>>(d_sim, s);
-  else k_eos_inv_fast<E, G><<<grid, KWB_THREADS, sm, st>>>(d_sim, s);
+  constexpr int B = Tiles<G>::BIG;
+  if (want_small(h, (long long)cdiv(h.N[1], 2 * B) * h.N[2])) eos_go<E, G, Tiles<G>::SMALL>(d_sim, h, fwd, s, st);
+  else eos_go<E, G, B>(d_sim, h, fwd, s, st);
   return cudaGetLastError();
+}
+
+template <int E, int G, int LT>
+static void spec_go(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s, cudaStream_t st) {
+  const int grid = cdiv(h.n1, LT) * (axis == 1 ? h.N[2] : h.N[1]);
+  k_spec_fast<E, G, LT><<<grid, LT * G, line_smem<E, G>(LT), st>>>(d_sim, axis, op, s);
 }
 
 template <int E, int G>
 static cudaError_t launch_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
                                cudaStream_t st) {
-  constexpr int L = KWB_THREADS / G;
-  const size_t sm = line_smem<E, G>(L);
-  const int grid = cdiv(h.n1, L) * (axis == 1 ? h.N[2] : h.N[1]);
-  k_spec_fast<E, G><<<grid, KWB_THREADS, sm, st>>>(d_sim, axis, op, s);
+  constexpr int B = Tiles<G>::BIG;
+  if (want_small(h, (long long)cdiv(h.n1, B) * (axis == 1 ? h.N[2] : h.N[1]))) spec_go<E, G, Tiles<G>::SMALL>(d_sim, h, axis, op, s, st);
+  else spec_go<E, G, B>(d_sim, h, axis, op, s, st);
   return cudaGetLastError();
 }
 

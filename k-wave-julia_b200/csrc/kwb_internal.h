@@ -102,6 +102,12 @@ struct SimDev {
   const long long *t0;  // device step base (CUDA graph replays advance it)
 
   int fast;  // register-FFT kernels (kwb_fast.cu) for power-of-two lines: bit 0 line passes, bit 1 EOS passes
+
+  // A dense (every-voxel) sensor group recording only pressure fields, updated by the x C2R
+  // pass as it writes p (no separate gather); nullptr when there is none.
+  const struct GroupDev *dense_p;
+
+  int num_sms;  // multiprocessors of the device (tile sizing)
 };
 
 // Sensor group on the device.

@@ -592,7 +592,7 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
 
 cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
                              long long step_s, cudaStream_t st) {
-  if ((h.fast & 1) && fast_size(h.N[axis])) return fast_line_pass(d_sim, h, axis, mode, step_s, st);
+  if ((h.fast & 1) && fast_size(h.N[axis]) && (axis == 0 || h.N[0] % 4 == 0)) return fast_line_pass(d_sim, h, axis, mode, step_s, st);
   const int L = h.L_line[axis];
   const size_t sm = line_pass_smem(h.N[axis], L);
   int tiles;
