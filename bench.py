@@ -163,6 +163,100 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def batch_bench(ctx, n_sims=64):
+    """Config 4: n mixed-size 2D simulations, batched (continuous batching, all submitted at once)
+    against one-at-a-time blocking solves of the same prepared problems.  Sims/s is measured
+    from the first submission to the last completion (host wall clock, device work inside)."""
+    import numpy as np
+    import kwave_b200 as kb
+    from kwave_b200 import workloads as W
+    cases = [W.c4_sim(i) for i in range(n_sims)]
+    vs = sum(c.voxels * c.Nt for c in cases)
+
+    def prep_all():
+        out = []
+        for c in cases:
+            g, m, s, sen, kw = c.to_api()
+            out.append(kb.prepare(g, m, s, sen, context=ctx, **kw))
+        return out
+
+    preps = prep_all()
+    kb.serving_config(max_running=64, chunk_steps=32, context=ctx)
+    t0 = time.perf_counter()
+    reqs = [kb.submit_prepared(p) for p in preps]
+    outs = [r.result() for r in reqs]
+    t_batch = time.perf_counter() - t0
+    st = kb.serving_stats(context=ctx)
+    preps1 = prep_all()
+    t0 = time.perf_counter()
+    alone = [kb.solve_prepared(p) for p in preps1]
+    t_one = time.perf_counter() - t0
+    same = all(np.array_equal(a["p"], b["p"]) for a, b in zip(alone, outs))
+    return {"workload": f"{n_sims} mixed-size 2D sims (sides 128-1024, Nt 500-4000, seeds 4004+i)",
+            "voxel_steps": vs, "batched_sims_per_s": n_sims / t_batch,
+            "one_at_a_time_sims_per_s": n_sims / t_one, "speedup": t_one / t_batch,
+            "batched_Gvoxel_steps_per_s": vs / t_batch / 1e9, "peak_running": st["peak_running"],
+            "results_identical_to_alone": bool(same)}
+
+
+def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800)):
+    """Config 5: Poisson arrivals (mean rate 200/s) of mixed 2D/3D requests; latency is arrival to
+    completion.  The comparison serves the same arrivals one at a time with blocking solves."""
+    import threading
+    import numpy as np
+    import kwave_b200 as kb
+    from kwave_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    cases = [W.c5_request(i, seed=seed, nt_range=nt_range) for i in range(n_req)]
+
+    def prep_all():
+        out = []
+        for c in cases:
+            g, m, s, sen, kw = c.to_api()
+            out.append(kb.prepare(g, m, s, sen, context=ctx, **kw))
+        return out
+
+    preps = prep_all()
+    kb.serving_config(max_running=64, chunk_steps=32, context=ctx)
+    reqs = [None] * n_req
+    t0 = time.perf_counter()
+
+    def feeder():
+        for i, p in enumerate(preps):
+            dt = t0 + arrivals[i] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            reqs[i] = (time.perf_counter(), kb.submit_prepared(p))
+
+    th = threading.Thread(target=feeder)
+    th.start()
+    th.join()
+    lat = []
+    for i in range(n_req):
+        ta, r = reqs[i]
+        r.result()
+        lat.append((r.info["end_ns"] - r.info["submit_ns"]) / 1e9)
+    t_end = max(t0 + arrivals[i] + lat[i] for i in range(n_req))
+    span = t_end - t0
+    preps1 = prep_all()
+    t0 = time.perf_counter()
+    lat1 = []
+    for i, p in enumerate(preps1):
+        dt = t0 + arrivals[i] - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        kb.solve_prepared(p)
+        lat1.append(time.perf_counter() - (t0 + arrivals[i]))
+    span1 = time.perf_counter() - t0
+    q = lambda a, x: float(np.percentile(np.asarray(a), x))
+    return {"workload": f"{n_req} Poisson requests at {rate:.0f}/s, 70% 2D 256-1024 / 30% 3D 64^3-192^3, "
+                        f"Nt {nt_range[0]}-{nt_range[1]}",
+            "sims_per_s": n_req / span, "p50_latency_s": q(lat, 50), "p99_latency_s": q(lat, 99),
+            "one_at_a_time": {"sims_per_s": n_req / span1, "p50_latency_s": q(lat1, 50),
+                              "p99_latency_s": q(lat1, 99)}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -172,6 +266,8 @@ def main():
     ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched (config 4) measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving (config 5) measurement")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -231,6 +327,9 @@ def main():
                "h2d_bytes_per_step": int(h2d / case.Nt), "d2h_bytes_per_step": int(d2h / case.Nt),
                "solve_s": el, "steps": case.Nt}
 
+    batch = None if args.no_batch else batch_bench(ctx)
+    serve = None if args.no_serve else serving_bench(ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, steps, el, cores = cpu_baseline(args.config)
@@ -253,6 +352,8 @@ def main():
                     "frac": spm_frac},
             "kernels": kernels,
             "e2e": e2e,
+            "batch": batch,
+            "serving": serve,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": info["launches_per_step"] * K + (K // 32),

@@ -193,6 +193,43 @@ int kwb_sim_profile(kwb_sim *sim, int64_t steps, kwb_kernel_times *out);
 /* Device bytes the simulation holds and kernels launched per time step. */
 int kwb_sim_info(const kwb_sim *sim, int64_t *device_bytes, int32_t *launches_per_step);
 
+/* Device bytes a simulation of `problem` would hold (what admission compares with free memory). */
+int kwb_estimate_device_bytes(kwb_ctx *ctx, const kwb_problem *problem, int64_t *bytes);
+
+/* ---- continuous batching: many independent simulations on one GPU ----------------------
+ * No counterpart in the reference (its solver runs one simulation per call on the host).
+ * Requests are admitted in submission order as slots and device memory allow, each admitted
+ * simulation keeps its fields resident and advances in CUDA-graph chunks on its own stream, so
+ * requests that arrive while others run overlap with them on the device.  `problem` (and every
+ * array it points to) and `outputs` must stay valid until kwb_wait() has returned for the ticket.
+ * The results are the same as kwb_solve's for the same problem. */
+typedef struct kwb_request_info {
+  int32_t status;                 /* the request's final status (KWB_OK, ...) */
+  int64_t submit_ns, start_ns, end_ns; /* steady-clock times: submitted, admitted, completed */
+  char error[256];
+} kwb_request_info;
+
+typedef struct kwb_serving_stats {
+  int64_t submitted, admitted, completed, failed, cancelled, chunks, peak_running;
+  int64_t queued, running, running_bytes;
+} kwb_serving_stats;
+
+/* Scheduler limits: at most `max_running` admitted simulations, `chunk_steps` time steps per
+ * launch, and (if > 0) at most `mem_cap_bytes` of modelled device memory in use. */
+int kwb_serving_config(kwb_ctx *ctx, int32_t max_running, int32_t chunk_steps, int64_t mem_cap_bytes);
+int kwb_submit(kwb_ctx *ctx, const kwb_problem *problem, kwb_outputs *outputs, uint64_t *ticket);
+/* *done = 1 once the request has completed (successfully or not). */
+int kwb_poll(kwb_ctx *ctx, uint64_t ticket, int32_t *done);
+/* Wait up to timeout_ns (< 0: forever); returns the request's status or KWB_E_TIMEOUT.  After a
+ * completed wait the ticket is released. */
+int kwb_wait(kwb_ctx *ctx, uint64_t ticket, int64_t timeout_ns, kwb_request_info *info);
+/* Ask a queued or running request to stop; it completes with KWB_E_CANCELLED. */
+int kwb_cancel(kwb_ctx *ctx, uint64_t ticket);
+int kwb_serving_stats_get(kwb_ctx *ctx, kwb_serving_stats *out);
+/* Submit n problems together and wait for all; status[i] per problem, returns the first error. */
+int kwb_solve_batch(kwb_ctx *ctx, int32_t n, const kwb_problem *const *problems,
+                    kwb_outputs *const *outputs, int32_t *status);
+
 /* ---- equation of state without device allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc -- hosts that own
  * all device memory through their own pool and forbid hidden allocations, real-time loops that

@@ -17,10 +17,16 @@
 #include "../../include/kwb.h"
 #include "kwb_internal.h"
 
+struct KwbServer;  // kwb_serve.cu
+
 struct kwb_ctx {
   int device = 0;
   std::string err;
+  KwbServer *server = nullptr;  // started by the first kwb_submit
 };
+
+size_t estimate_device_bytes(const kwb_problem *P);
+void kwb_server_shutdown(kwb_ctx *ctx);
 
 static std::string g_create_err;
 static const double kPi = 3.141592653589793238462643;
@@ -127,6 +133,7 @@ struct GroupHost {
   GroupDev dev{};
   GroupDev *d_dev = nullptr;
   long long n = 0;
+  bool fused = false;  // updated inside the x C2R pass
 };
 
 struct kwb_sim {
@@ -332,7 +339,7 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
   }
   if ((e = launch_eos_x_inv(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
   for (auto &g : S->groups) {
-    if (g.spec.cartesian || g.n == 0) continue;
+    if (g.spec.cartesian || g.n == 0 || g.fused) continue;
     if ((e = launch_sensor_gather(S->d_sim, h, g.d_dev, g.n, step_s, st)) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -341,11 +348,46 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
 int count_launches(const kwb_sim *S) {
   int n = (S->tr ? 1 : 0) + S->h.ndim + 2 + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? 3 : 0));
   for (auto &g : S->groups)
-    if (!g.spec.cartesian && g.n > 0) ++n;
+    if (!g.spec.cartesian && g.n > 0 && !g.fused) ++n;
   return n;
 }
 
 }  // namespace
+
+// Device bytes a simulation of `P` holds (fields, spectra, medium, tables, sensor buffers and
+// the FP64 upload staging), the figure admission control compares with free memory.
+size_t estimate_device_bytes(const kwb_problem *P) {
+  const int D = P->ndim;
+  long long N[3] = {1, 1, 1};
+  for (int a = 0; a < D; ++a) N[a] = P->N[a];
+  const long long nvox = N[0] * N[1] * N[2];
+  const long long nspec = (N[0] / 2 + 1) * N[1] * N[2];
+  const bool c_arr = P->c0.count == nvox && nvox > 1;
+  const bool r_arr = P->rho0.count == nvox && nvox > 1;
+  const bool b_arr = P->BonA.count == nvox && nvox > 1;
+  const bool nonlinear = P->BonA.count > 0;
+  const bool dispersion = !c_arr && P->alpha_mode == KWB_STOKES;
+  size_t need = (size_t)nvox * 4 * (1 + 2 * D) + (size_t)nspec * 8;
+  if (dispersion) need += (size_t)nvox * 4 + (size_t)nspec * 8;
+  need += (size_t)nspec * 4 * (dispersion ? 2 : 1);
+  need += (size_t)nvox * 4 * ((r_arr ? 1 : 0) + (c_arr ? 1 : 0) + ((nonlinear && (b_arr || r_arr)) ? 1 : 0));
+  if (c_arr || r_arr || b_arr || P->p0.count) need += (size_t)nvox * 8 * ((nonlinear && b_arr && r_arr) ? 2 : 1);
+  for (int g = 0; g < P->n_groups; ++g) {
+    const kwb_sensor_group &G = P->groups[g];
+    if (G.cartesian) continue;
+    const long long n = G.dense ? nvox : G.n_index;
+    for (int f = 0; f < KWB_REC_COUNT; ++f)
+      if (G.record_mask & (1u << f)) {
+        const bool series = f == KWB_REC_P || f == KWB_REC_UX || f == KWB_REC_UY || f == KWB_REC_UZ;
+        need += (size_t)n * (series ? (size_t)P->Nt * 4 : 8);
+      }
+  }
+  if (P->n_p_index > 0) need += (size_t)P->p_signal.n_rows * P->p_signal.n_cols * 12;
+  for (int d = 0; d < 3; ++d)
+    if (P->u_signal[d].data) need += (size_t)P->u_signal[d].n_rows * P->u_signal[d].n_cols * 12;
+  if (P->tr.data) need += (size_t)P->tr.n_rows * P->tr.n_cols * 12;
+  return need + (size_t)16 * 1024 * 1024;  // per-axis tables, CSR lists, descriptor, slack
+}
 
 // =============================================================================================
 // C ABI
@@ -385,7 +427,11 @@ int kwb_context_create(int device, kwb_ctx **out) {
   return KWB_OK;
 }
 
-void kwb_context_destroy(kwb_ctx *ctx) { delete ctx; }
+void kwb_context_destroy(kwb_ctx *ctx) {
+  if (!ctx) return;
+  kwb_server_shutdown(ctx);
+  delete ctx;
+}
 
 const char *kwb_last_error(const kwb_ctx *ctx) {
   return ctx ? ctx->err.c_str() : g_create_err.c_str();
@@ -474,21 +520,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
 
   // ---- admission by free device memory
   {
-    size_t need = (size_t)nvox * 4 * (1 + 2 * D) + (size_t)h.nspec * 8;
-    if (h.dispersion) need += (size_t)nvox * 4 + (size_t)h.nspec * 8;
-    need += (size_t)h.nspec * 4 * (h.dispersion ? 2 : 1);
-    need += (size_t)nvox * 4 * ((r_arr ? 1 : 0) + (c_arr ? 1 : 0) + ((nonlinear && (b_arr || r_arr)) ? 1 : 0));
-    need += (size_t)nvox * 8;  // FP64 staging for medium uploads
-    for (int g = 0; g < P->n_groups; ++g) {
-      const kwb_sensor_group &G = P->groups[g];
-      if (G.cartesian) continue;
-      const long long n = G.dense ? nvox : G.n_index;
-      for (int f = 0; f < KWB_REC_COUNT; ++f)
-        if (G.record_mask & (1u << f)) {
-          const bool series = f == KWB_REC_P || f == KWB_REC_UX || f == KWB_REC_UY || f == KWB_REC_UZ;
-          need += (size_t)n * (series ? (size_t)P->Nt * 4 : 8);
-        }
-    }
+    const size_t need = estimate_device_bytes(P);
     size_t free_b = 0, total_b = 0;
     CU(cudaMemGetInfo(&free_b, &total_b));
     if (need + (size_t)64 * 1024 * 1024 > free_b)
@@ -745,6 +777,19 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     }
   }
 
+  // ---- a dense pressure-only sensor group is updated inside the fast x C2R pass
+  {
+    const unsigned ponly = (1u << KWB_REC_P) | (1u << KWB_REC_P_MAX) | (1u << KWB_REC_P_MIN) |
+                           (1u << KWB_REC_P_RMS) | (1u << KWB_REC_P_FINAL);
+    const bool fast_inv = (h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0]);
+    for (auto &G : S->groups) {
+      if (!fast_inv || G.spec.cartesian || !G.dev.dense || G.n == 0 || (G.dev.mask & ~ponly)) continue;
+      h.dense_p = G.d_dev;
+      G.fused = true;
+      break;
+    }
+  }
+  CU(cudaDeviceGetAttribute(&h.num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
   CU(prime_attributes(h));
 
   // ---- device descriptor
@@ -924,6 +969,24 @@ void kwb_sim_destroy(kwb_sim *S) {
   delete S;
 }
 
+}  // extern "C"
+
+// accessors for the serving scheduler (kwb_serve.cu)
+cudaStream_t kwb_sim_stream_of(kwb_sim *S) { return S->stream; }
+long long kwb_sim_nt_of(const kwb_sim *S) { return S->Nt_loop; }
+void kwb_ctx_set_err(kwb_ctx *ctx, const char *msg) { ctx->err = msg ? msg : ""; }
+int kwb_ctx_device(const kwb_ctx *ctx) { return ctx->device; }
+KwbServer *&kwb_ctx_server_slot(kwb_ctx *ctx) { return ctx->server; }
+
+extern "C" {
+
+int kwb_estimate_device_bytes(kwb_ctx *ctx, const kwb_problem *P, int64_t *bytes) {
+  int rc = validate_problem(ctx, P);
+  if (rc) return rc;
+  if (bytes) *bytes = (int64_t)estimate_device_bytes(P);
+  return KWB_OK;
+}
+
 int kwb_sim_info(const kwb_sim *S, int64_t *device_bytes, int32_t *launches_per_step) {
   if (!S) return KWB_E_INVALID;
   if (device_bytes) *device_bytes = (int64_t)S->mem.bytes;
@@ -1001,7 +1064,7 @@ int kwb_sim_profile(kwb_sim *S, int64_t steps, kwb_kernel_times *out) {
     }
     timed(slot("eos_x_inv", ns * 8.0 + nv * 4.0 + (h.ndim == 1 ? ns * 4.0 : 0.0)), [&] { return launch_eos_x_inv(S->d_sim, h, s, st); });
     for (auto &g : S->groups) {
-      if (g.spec.cartesian || g.n == 0) continue;
+      if (g.spec.cartesian || g.n == 0 || g.fused) continue;
       timed(slot("sensor_gather", 0.0), [&] { return launch_sensor_gather(S->d_sim, h, g.d_dev, g.n, s, st); });
     }
     S->steps_done++;

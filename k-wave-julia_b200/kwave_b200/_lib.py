@@ -92,6 +92,16 @@ class KernelTimes(C.Structure):
                 ("launches", C.c_int64 * 16), ("bytes_per_launch", C.c_double * 16)]
 
 
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("submit_ns", C.c_int64), ("start_ns", C.c_int64),
+                ("end_ns", C.c_int64), ("error", C.c_char * 256)]
+
+
+class ServingStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "admitted", "completed", "failed", "cancelled",
+                                          "chunks", "peak_running", "queued", "running", "running_bytes")]
+
+
 EXPORTS = (
     "kwb_version", "kwb_context_create", "kwb_context_destroy", "kwb_last_error",
     "kwb_query_outputs", "kwb_solve", "kwb_sim_create", "kwb_sim_advance",
@@ -147,6 +157,20 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         lib.kwb_sim_profile.argtypes = [vp, C.c_int64, C.POINTER(KernelTimes)]
         lib.kwb_sim_info.restype = C.c_int
         lib.kwb_sim_info.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        lib.kwb_estimate_device_bytes.restype = C.c_int
+        lib.kwb_estimate_device_bytes.argtypes = [vp, C.POINTER(Problem), C.POINTER(C.c_int64)]
+        lib.kwb_serving_config.restype = C.c_int
+        lib.kwb_serving_config.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64]
+        lib.kwb_submit.restype = C.c_int
+        lib.kwb_submit.argtypes = [vp, C.POINTER(Problem), C.POINTER(Outputs), C.POINTER(C.c_uint64)]
+        lib.kwb_poll.restype = C.c_int
+        lib.kwb_poll.argtypes = [vp, C.c_uint64, C.POINTER(C.c_int32)]
+        lib.kwb_wait.restype = C.c_int
+        lib.kwb_wait.argtypes = [vp, C.c_uint64, C.c_int64, C.POINTER(RequestInfo)]
+        lib.kwb_cancel.restype = C.c_int
+        lib.kwb_cancel.argtypes = [vp, C.c_uint64]
+        lib.kwb_serving_stats_get.restype = C.c_int
+        lib.kwb_serving_stats_get.argtypes = [vp, C.POINTER(ServingStats)]
         _lib = lib
         return lib
 

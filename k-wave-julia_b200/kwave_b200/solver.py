@@ -452,3 +452,135 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------------------------
+# continuous batching (kwb_submit / kwb_wait): many independent simulations on one GPU
+# ---------------------------------------------------------------------------------------------
+
+class Request:
+    """A submitted simulation; keeps every host array the C side reads or writes alive."""
+
+    def __init__(self, ctx, ticket, built, O, outs, arrays, pfull, kgrid, sensor, Nt):
+        self.ctx, self.ticket = ctx, ticket
+        self._keep = (built, O, outs, arrays, pfull)
+        self.kgrid, self.sensor, self.Nt = kgrid, sensor, Nt
+        self._result = None
+        self.info = None
+
+    def done(self) -> bool:
+        if self._result is not None or self.info is not None:
+            return True
+        d = C.c_int32(0)
+        check(self.ctx.lib, self.ctx.handle, self.ctx.lib.kwb_poll(self.ctx.handle, self.ticket, C.byref(d)))
+        return bool(d.value)
+
+    def result(self, timeout: Optional[float] = None) -> SimulationOutput:
+        if self._result is not None:
+            return self._result
+        if self.info is not None:
+            raise KWaveB200Error(self.info["status"], self.info["error"])
+        info = _lib.RequestInfo()
+        t = -1 if timeout is None else int(timeout * 1e9)
+        rc = self.ctx.lib.kwb_wait(self.ctx.handle, self.ticket, t, C.byref(info))
+        if rc == _lib.KWB_E_TIMEOUT:
+            raise TimeoutError(f"request {self.ticket} still running")
+        self.info = dict(status=info.status, submit_ns=info.submit_ns, start_ns=info.start_ns,
+                         end_ns=info.end_ns, error=info.error.decode())
+        if rc != _lib.KWB_OK:
+            raise KWaveB200Error(rc, self.info["error"])
+        built, O, outs, arrays, pfull = self._keep
+        self._result = _collect(built, arrays, pfull, self.sensor, self.kgrid, self.Nt)
+        return self._result
+
+    def cancel(self):
+        check(self.ctx.lib, self.ctx.handle, self.ctx.lib.kwb_cancel(self.ctx.handle, self.ticket))
+
+    @property
+    def latency_s(self) -> Optional[float]:
+        return None if self.info is None else (self.info["end_ns"] - self.info["submit_ns"]) / 1e9
+
+
+class Prepared:
+    """A problem packed for the C ABI with its output buffers (host work done ahead of time)."""
+
+    def __init__(self, ctx, kgrid, sensor, built):
+        self.ctx, self.kgrid, self.sensor, self.built = ctx, kgrid, sensor, built
+        self.Nt = int(built.problem.tr.n_cols if built.problem.tr.data else built.problem.Nt)
+        self.O, self.outs, self.arrays, self.pfull = _alloc_outputs(ctx, built, kgrid)
+
+    @property
+    def voxels(self) -> int:
+        return int(np.prod(self.kgrid.N))
+
+
+def prepare(kgrid, medium, source, sensor, *, pml_size=20, pml_alpha=2.0, smooth_p0=True,
+            extra_sensors=(), context: Optional[Context] = None) -> Prepared:
+    ctx = context or default_context()
+    b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
+                      smooth_p0=smooth_p0, extra_sensors=extra_sensors)
+    return Prepared(ctx, kgrid, sensor, b)
+
+
+def submit_prepared(prep: Prepared) -> Request:
+    ctx = prep.ctx
+    t = C.c_uint64(0)
+    check(ctx.lib, ctx.handle, ctx.lib.kwb_submit(ctx.handle, C.byref(prep.built.problem), C.byref(prep.O), C.byref(t)))
+    return Request(ctx, t.value, prep.built, prep.O, prep.outs, prep.arrays, prep.pfull, prep.kgrid,
+                   prep.sensor, prep.Nt)
+
+
+def solve_prepared(prep: Prepared) -> SimulationOutput:
+    """The plain one-at-a-time path: a blocking kwb_solve of a prepared problem."""
+    ctx = prep.ctx
+    with ctx.lock:
+        check(ctx.lib, ctx.handle, ctx.lib.kwb_solve(ctx.handle, C.byref(prep.built.problem), C.byref(prep.O)))
+    return _collect(prep.built, prep.arrays, prep.pfull, prep.sensor, prep.kgrid, prep.Nt)
+
+
+def submit(kgrid, medium, source, sensor, *, pml_size=20, pml_alpha=2.0, smooth_p0=True,
+           extra_sensors=(), context: Optional[Context] = None) -> Request:
+    """Queue one simulation for continuous batching; returns a Request (non-blocking)."""
+    return submit_prepared(prepare(kgrid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
+                                   smooth_p0=smooth_p0, extra_sensors=extra_sensors, context=context))
+
+
+def serving_config(max_running: int = 64, chunk_steps: int = 32, mem_cap_bytes: int = 0,
+                   context: Optional[Context] = None):
+    ctx = context or default_context()
+    check(ctx.lib, ctx.handle, ctx.lib.kwb_serving_config(ctx.handle, max_running, chunk_steps, mem_cap_bytes))
+
+
+def serving_stats(context: Optional[Context] = None) -> dict:
+    ctx = context or default_context()
+    st = _lib.ServingStats()
+    check(ctx.lib, ctx.handle, ctx.lib.kwb_serving_stats_get(ctx.handle, C.byref(st)))
+    return {n: getattr(st, n) for n, _ in st._fields_}
+
+
+def estimate_device_bytes(kgrid, medium, source, sensor, context: Optional[Context] = None, **kw) -> int:
+    ctx = context or default_context()
+    b = build_problem(kgrid, medium, source, sensor, **kw)
+    v = C.c_int64(0)
+    check(ctx.lib, ctx.handle, ctx.lib.kwb_estimate_device_bytes(ctx.handle, C.byref(b.problem), C.byref(v)))
+    return v.value
+
+
+def solve_batch(jobs, context: Optional[Context] = None) -> list:
+    """Run many independent simulations together; jobs are (kgrid, medium, source, sensor, kwargs)."""
+    reqs = [submit(g, m, s, sen, context=context, **kw) for g, m, s, sen, kw in jobs]
+    return [r.result() for r in reqs]
+
+
+def shard_jobs(costs, world: int, rank: int) -> list:
+    """Indices of the jobs rank `rank` runs when `world` GPUs share a batch: longest-processing-
+    time-first greedy assignment on the given costs (e.g. voxels x steps).  Simulations are
+    independent, so ranks exchange nothing while they run."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    owner = [0] * len(costs)
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += costs[i]
+    return [i for i in range(len(costs)) if owner[i] == rank]
