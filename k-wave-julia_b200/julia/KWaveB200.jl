@@ -1,0 +1,253 @@
+"""
+    KWaveB200
+
+Runs KWave.jl's fluid k-space time stepping on an NVIDIA B200 through libkwb's C ABI
+(`include/kwb.h`).  `KWaveB200.kspace_first_order` has the signature and output of
+`KWave.kspace_first_order` (KWave.jl/src/solver/first_order.jl:92-111, 287-306, 505-524):
+
+    using KWave, KWaveB200
+    out = KWaveB200.kspace_first_order(kgrid, medium, source, sensor; pml_size=20, smooth_p0=true)
+
+or, to switch every call site at once, `import KWaveB200: kspace_first_order` after `using KWave`.
+
+The host side stays in Julia: the shim normalises the keyword arguments exactly where the
+reference does, smooths p0 with `KWave.smooth(p0; restore_max=true)` in Float64 (as
+initialize_p0_*! does), passes column-major arrays and `findall` indices (minus one) to the
+library, and returns a `KWave.SimulationOutput` of Float64 arrays.  Fields and FFTs run in FP32
+on the GPU whatever `data_cast` says.  libkwb.so is found at `ENV["KWB_LIBRARY"]` or next to the
+Python host package (`k-wave-julia_b200/kwave_b200/libkwb.so`).
+"""
+module KWaveB200
+
+using KWave
+
+const libkwb = get(ENV, "KWB_LIBRARY", joinpath(@__DIR__, "..", "kwave_b200", "libkwb.so"))
+
+const REC = Dict(:p => 0, :p_max => 1, :p_min => 2, :p_rms => 3, :p_final => 4, :ux => 5,
+                 :uy => 6, :uz => 7, :u_max => 8, :u_rms => 9, :u_final => 10, :I_avg => 11,
+                 :I_max => 12)
+const SERIES = (:p, :ux, :uy, :uz)
+
+struct KwbField
+    data::Ptr{Float64}
+    count::Int64
+end
+struct KwbSignal
+    data::Ptr{Float64}
+    n_rows::Int64
+    n_cols::Int64
+end
+struct KwbSensorGroup
+    index::Ptr{Int64}
+    n_index::Int64
+    dense::Int32
+    cartesian::Int32
+    record_mask::UInt32
+    record_count::NTuple{13,UInt8}
+end
+struct KwbProblem
+    ndim::Int32
+    N::NTuple{3,Int64}
+    d::NTuple{3,Float64}
+    dt::Float64
+    Nt::Int64
+    pml_size::NTuple{3,Int64}
+    pml_alpha::NTuple{3,Float64}
+    c0::KwbField
+    rho0::KwbField
+    BonA::KwbField
+    alpha_mode::Int32
+    alpha_coeff::Float64
+    alpha_power::Float64
+    p0::KwbField
+    p_index::Ptr{Int64}
+    n_p_index::Int64
+    p_mode::Int32
+    p_signal::KwbSignal
+    u_index::Ptr{Int64}
+    n_u_index::Int64
+    u_mode::Int32
+    u_signal::NTuple{3,KwbSignal}
+    tr::KwbSignal
+    n_groups::Int32
+    groups::Ptr{KwbSensorGroup}
+    progress::Ptr{Cvoid}
+    progress_user::Ptr{Cvoid}
+end
+struct KwbGroupSizes
+    rows::NTuple{13,Int64}
+    cols::NTuple{13,Int64}
+end
+struct KwbGroupOutputs
+    field::NTuple{13,Ptr{Float64}}
+end
+struct KwbOutputs
+    groups::Ptr{KwbGroupOutputs}
+    p_final_full::Ptr{Float64}
+end
+
+const CTX = Ref{Ptr{Cvoid}}(C_NULL)
+
+function context()
+    if CTX[] == C_NULL
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:kwb_context_create, libkwb), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h)
+        rc == 0 || error(unsafe_string(ccall((:kwb_last_error, libkwb), Cstring, (Ptr{Cvoid},), C_NULL)))
+        CTX[] = h[]
+    end
+    return CTX[]
+end
+
+check(rc) = rc == 0 ? rc :
+    error(unsafe_string(ccall((:kwb_last_error, libkwb), Cstring, (Ptr{Cvoid},), context())))
+
+# a scalar or array medium property (count 0 = nothing)
+function field(x, keep)
+    x === nothing && return KwbField(C_NULL, 0)
+    v = x isa Real ? Float64[x] : vec(Float64.(x))   # column-major, like the reference
+    push!(keep, v)
+    return KwbField(pointer(v), length(v))
+end
+
+function signal(s, keep)
+    s === nothing && return KwbSignal(C_NULL, 0, 0)
+    m = s isa AbstractVector ? reshape(Float64.(s), :, 1) : Float64.(s)  # a Vector acts as n x 1
+    push!(keep, m)
+    return KwbSignal(pointer(m), size(m, 1), size(m, 2))
+end
+
+function indices(mask, keep)
+    idx = Int64.(LinearIndices(mask)[findall(mask)]) .- 1
+    push!(keep, idx)
+    return idx
+end
+
+const _ALPHA = Dict(:no_absorption => 0, :no_dispersion => 1, :stokes => 2)
+
+function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, data_cast,
+                progress_callback)
+    (kgrid.Nt[] == 0 || kgrid.dt[] == 0) &&
+        error("Time array not set. Call make_time!(kgrid, sound_speed) before running.")
+    KWave.validate_record_fields(sensor)
+    dims = KWave.grid_size(kgrid)
+    D = length(dims)
+    ds = KWave.grid_spacing(kgrid)
+    keep = Any[]
+    psz = pml_size isa Tuple ? pml_size : ntuple(_ -> pml_size, D)
+    pal = pml_alpha isa Tuple ? pml_alpha : ntuple(_ -> pml_alpha, D)
+    pad3(t, v) = ntuple(i -> i <= D ? t[i] : v, 3)
+
+    lossless = KWave.is_lossless(medium)
+    if !lossless && !(medium.alpha_coeff isa Real)
+        error("array alpha_coeff is not supported")          # T(absorb_tau) raises in the reference
+    end
+    tr = KWave.is_time_reversal(sensor)
+    p0 = KwbField(C_NULL, 0)
+    if KWave.has_p0(source) && !tr
+        q = Float64.(Array(source.p0))
+        if smooth_p0 && ((D == 1 && dims[1] > 4) || (D > 1 && all(>(1), dims)))
+            q = KWave.smooth(q; restore_max=true)
+        end
+        p0 = field(q, keep)
+    end
+    p_idx = KWave.has_pressure_source(source) ? indices(source.p_mask, keep) : Int64[]
+    u_idx = KWave.has_velocity_source(source) ? indices(source.u_mask, keep) : Int64[]
+    psig = KWave.has_pressure_source(source) ? signal(source.p, keep) : KwbSignal(C_NULL, 0, 0)
+    usig = (signal(source.ux, keep), D > 1 ? signal(source.uy, keep) : KwbSignal(C_NULL, 0, 0),
+            D > 2 ? signal(source.uz, keep) : KwbSignal(C_NULL, 0, 0))
+
+    groups = KwbSensorGroup[]
+    if sensor.mask !== nothing
+        counts = zeros(UInt8, 13)
+        mask = 0x00000000
+        for f in sensor.record
+            mask |= UInt32(1) << REC[f]
+            counts[REC[f] + 1] += 1
+        end
+        if (:I_avg in sensor.record || :I_max in sensor.record) && data_cast == Float32 &&
+           sensor.mask isa AbstractArray{Bool}
+            throw(MethodError(KWave._acoustic_intensity, (0.0f0,)))
+        end
+        if sensor.mask isa AbstractArray{Bool}
+            idx = indices(sensor.mask, keep)
+            dense = length(idx) == prod(dims)
+            push!(groups, KwbSensorGroup(dense ? C_NULL : pointer(idx), length(idx), Int32(dense), 0,
+                                         mask, Tuple(counts)))
+        else
+            push!(groups, KwbSensorGroup(C_NULL, size(sensor.mask, 2), 0, 1, mask, Tuple(counts)))
+        end
+    end
+    push!(keep, groups)
+    trs = tr ? signal(sensor.time_reversal_boundary_data, keep) : KwbSignal(C_NULL, 0, 0)
+
+    cb = C_NULL
+    if progress_callback !== nothing
+        fn = (t::Int64, Nt::Int64, p::Ptr{Float32}, ::Ptr{Cvoid}) ->
+            (progress_callback(t, Nt, reshape(copy(unsafe_wrap(Array, p, prod(dims))), dims)); nothing)
+        cfn = @cfunction($fn, Cvoid, (Int64, Int64, Ptr{Float32}, Ptr{Cvoid}))
+        push!(keep, cfn)
+        cb = Base.unsafe_convert(Ptr{Cvoid}, cfn)
+    end
+
+    P = Ref(KwbProblem(Int32(D), pad3(dims, 1), pad3(ds, 1.0), kgrid.dt[], kgrid.Nt[],
+                       pad3(psz, 0), pad3(Float64.(pal), 0.0),
+                       field(medium.sound_speed, keep), field(medium.density, keep),
+                       field(medium.BonA, keep),
+                       lossless ? 0 : _ALPHA[medium.alpha_mode],
+                       lossless ? 0.0 : Float64(medium.alpha_coeff),
+                       lossless ? 0.0 : Float64(medium.alpha_power), p0,
+                       isempty(p_idx) ? C_NULL : pointer(p_idx), length(p_idx), Int32(Int(source.p_mode)), psig,
+                       isempty(u_idx) ? C_NULL : pointer(u_idx), length(u_idx), Int32(Int(source.u_mode)), usig,
+                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL))
+    ctx = context()
+    GC.@preserve keep begin
+        sizes = Vector{KwbGroupSizes}(undef, max(length(groups), 1))
+        pf_len = Ref{Int64}(0)
+        check(ccall((:kwb_query_outputs, libkwb), Cint,
+                    (Ptr{Cvoid}, Ref{KwbProblem}, Ptr{KwbGroupSizes}, Ref{Int64}), ctx, P, sizes, pf_len))
+        data = Dict{Symbol,AbstractArray}()
+        outs = KwbGroupOutputs[]
+        if !isempty(groups)
+            ptrs = fill(Ptr{Float64}(C_NULL), 13)
+            for f in unique(sensor.record)
+                i = REC[f]
+                a = zeros(Float64, sizes[1].rows[i + 1], sizes[1].cols[i + 1])
+                data[f] = f in SERIES ? a : vec(a)
+                ptrs[i + 1] = pointer(a)
+            end
+            push!(outs, KwbGroupOutputs(Tuple(ptrs)))
+        end
+        pfull = zeros(Float64, pf_len[])
+        O = Ref(KwbOutputs(isempty(outs) ? C_NULL : pointer(outs), pf_len[] > 0 ? pointer(pfull) : C_NULL))
+        GC.@preserve data outs pfull begin
+            check(ccall((:kwb_solve, libkwb), Cint, (Ptr{Cvoid}, Ref{KwbProblem}, Ref{KwbOutputs}), ctx, P, O))
+        end
+    end
+    if tr
+        kgrid.Nt[] = size(sensor.time_reversal_boundary_data, 2)   # first_order.jl:430-431
+        data[:p_final] = pfull
+    end
+    KWave.apply_sensor_directivity!(data, sensor, kgrid)            # host post-filters, as the
+    KWave.apply_frequency_response!(data, sensor, kgrid)            # reference runs them
+    return KWave.SimulationOutput(data)
+end
+
+"""
+    kspace_first_order(kgrid, medium, source, sensor; kwargs...) -> SimulationOutput
+
+Same arguments and output as `KWave.kspace_first_order`; the time loop runs on the GPU.
+`pml_inside`, `smooth_c0`, `smooth_rho0`, `plot_*`, `record_movie` and `show_progress` are
+accepted and ignored, as in the reference solver body; `save_to_disk` is not supported.
+"""
+function kspace_first_order(kgrid::KWave.AbstractKWaveGrid, medium::KWave.KWaveMedium,
+                            source::KWave.KWaveSource, sensor::KWave.KWaveSensor;
+                            pml_inside::Bool=true, pml_size=20, pml_alpha=2.0, smooth_p0::Bool=true,
+                            smooth_c0::Bool=false, smooth_rho0::Bool=false,
+                            data_cast::Type{T}=Float64, save_to_disk=nothing, plot_sim::Bool=false,
+                            plot_layout::Symbol=:default, plot_scale=:auto, record_movie=nothing,
+                            progress_callback=nothing, show_progress::Bool=true) where {T<:AbstractFloat}
+    save_to_disk === nothing || error("save_to_disk (HDF5 input files) is not supported by KWaveB200")
+    return _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, T, progress_callback)
+end
+
+end # module
