@@ -508,6 +508,11 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (fp && strcmp(fp, "generic") == 0) h.fast = 0;
     if (fp && strcmp(fp, "line") == 0) h.fast = 1;
     if (fp && strcmp(fp, "eos") == 0) h.fast = 2;
+    const char *tv = getenv("KWB_TILE");
+    h.tile_override = -1;
+    if (tv && strcmp(tv, "big") == 0) h.tile_override = 0;
+    if (tv && strcmp(tv, "mid") == 0) h.tile_override = 1;
+    if (tv && strcmp(tv, "small") == 0) h.tile_override = 2;
   }
 
   // ---- tile shapes and FFT plans

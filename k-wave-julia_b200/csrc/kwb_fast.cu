@@ -86,8 +86,9 @@ __device__ __forceinline__ float2 cmul_conj(float2 a, float2 w) {  // a * conj(w
 
 // N = E*G point transform of the line owned by this thread's group.  xs: the line's exchange
 // buffer (E rows of pitch G+1); tw2: exp(-2 pi i t q/N) at [q*(G+1) + t].
-template <int E, int G, bool WARP>
+template <int E_, int G_, bool WARP>
 struct LineFFT {
+  static constexpr int E = E_, G = G_;
   static constexpr int N = E * G, J = E / G, RP = G + 1, LP = E * RP + 1;
   static_assert(E % G == 0, "G must divide E");
   __device__ __forceinline__ static void sync() {
@@ -131,6 +132,122 @@ struct LineFFT {
   }
   // frequency index held in register idx by thread t
   __device__ __forceinline__ static int k_of(int t, int idx) { return t * J + idx / G + E * (idx % G); }
+  // per-CTA twiddle table: exp(-2 pi i t q/N) at [q*(G+1) + t]
+  static constexpr int TW = E * RP;
+  __device__ __forceinline__ static void build_tw(float2 *tw2, const float2 *tw) {
+    for (int e = threadIdx.x; e < E * G; e += blockDim.x) {
+      const int q = e / G, u = e - q * G;
+      tw2[q * RP + u] = tw[u * q];
+    }
+  }
+};
+
+// N = R1 * A * B point transform of one line owned by G = A*B threads, each holding E = R1
+// elements (three levels, two shared-memory exchanges): an R1-point DFT in registers over
+// x[t + G r]; twiddle exp(-2 pi i t q1/N); exchange; for each (q1, a) a B-point DFT over b of
+// the values at t = a + A b, twiddle exp(-2 pi i a m_b/G); exchange; for each (q1, m_b) an
+// A-point DFT over a, giving X[q1 + R1 (m_b + B m_a)].  Fewer registers per thread than the
+// two-level form (E = 8 for N = 128..512), so twice the resident warps.
+template <int R1, int A, int B, bool WARP>
+struct LineFFT3 {
+  static constexpr int E = R1, G = A * B, N = R1 * A * B;
+  static constexpr int P2 = R1 / B, P3 = R1 / A;  // (q1, a) and (q1, m_b) pairs per thread
+  static_assert(R1 % A == 0 && R1 % B == 0, "A and B must divide R1");
+  static constexpr int RP = G + 1;                 // pitch of the [q1][t] layout
+  static constexpr int AP = A + 1;                 // pitch of the [q1][m_b][a] layout
+  static constexpr int S1 = R1 * RP, S2 = R1 * B * AP;
+  static constexpr int LP = (S1 > S2 ? S1 : S2) + 1;
+  static constexpr int TW = R1 * RP + B * AP;      // level-1 then level-2 twiddles
+  __device__ __forceinline__ static void sync() {
+    if (WARP) __syncwarp();
+    else __syncthreads();
+  }
+  __device__ __forceinline__ static void build_tw(float2 *tw, const float2 *g) {
+    for (int e = threadIdx.x; e < R1 * G; e += blockDim.x) {
+      const int q = e / G, u = e - q * G;
+      tw[q * RP + u] = g[u * q];  // exp(-2 pi i u q / N)
+    }
+    for (int e = threadIdx.x; e < A * B; e += blockDim.x) {
+      const int mb = e / A, a = e - mb * A;
+      tw[R1 * RP + mb * AP + a] = g[a * mb * R1];  // exp(-2 pi i a m_b / G)
+    }
+  }
+  // in: v[r] = x[t + G r]; out: v[j*A + m_a] = X[q1 + R1 (m_b + B m_a)], (q1, m_b) = pair t*P3 + j
+  __device__ __forceinline__ static void fwd(float2 (&v)[E], float2 *xs, const float2 *tw, int t) {
+    dft_reg<R1, false>(v);
+#pragma unroll
+    for (int q = 0; q < R1; ++q) xs[q * RP + t] = cmul(v[q], tw[q * RP + t]);
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
+      float2 w[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) w[b] = xs[q1 * RP + a + A * b];
+      dft_reg<B, false>(w);
+#pragma unroll
+      for (int mb = 0; mb < B; ++mb) v[j * B + mb] = cmul(w[mb], tw[R1 * RP + mb * AP + a]);
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
+#pragma unroll
+      for (int mb = 0; mb < B; ++mb) xs[(q1 * B + mb) * AP + a] = v[j * B + mb];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P3; ++j) {
+      const int p = t * P3 + j, q1 = p / B, mb = p - q1 * B;
+      float2 w[A];
+#pragma unroll
+      for (int a = 0; a < A; ++a) w[a] = xs[(q1 * B + mb) * AP + a];
+      dft_reg<A, false>(w);
+#pragma unroll
+      for (int ma = 0; ma < A; ++ma) v[j * A + ma] = w[ma];
+    }
+    sync();
+  }
+  // exact reverse of fwd with conjugate twiddles (unnormalised); out: v[r] = x[t + G r]
+  __device__ __forceinline__ static void inv(float2 (&v)[E], float2 *xs, const float2 *tw, int t) {
+#pragma unroll
+    for (int j = 0; j < P3; ++j) {
+      const int p = t * P3 + j, q1 = p / B, mb = p - q1 * B;
+      float2 w[A];
+#pragma unroll
+      for (int ma = 0; ma < A; ++ma) w[ma] = v[j * A + ma];
+      dft_reg<A, true>(w);
+#pragma unroll
+      for (int a = 0; a < A; ++a) xs[(q1 * B + mb) * AP + a] = w[a];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
+      float2 w[B];
+#pragma unroll
+      for (int mb = 0; mb < B; ++mb) w[mb] = cmul_conj(xs[(q1 * B + mb) * AP + a], tw[R1 * RP + mb * AP + a]);
+      dft_reg<B, true>(w);
+#pragma unroll
+      for (int b = 0; b < B; ++b) v[j * B + b] = w[b];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
+#pragma unroll
+      for (int b = 0; b < B; ++b) xs[q1 * RP + a + A * b] = v[j * B + b];
+    }
+    sync();
+#pragma unroll
+    for (int q = 0; q < R1; ++q) v[q] = cmul_conj(xs[q * RP + t], tw[q * RP + t]);
+    dft_reg<R1, true>(v);
+    sync();
+  }
+  __device__ __forceinline__ static int k_of(int t, int idx) {
+    const int p = t * P3 + idx / A, q1 = p / B, mb = p - q1 * B, ma = idx % A;
+    return q1 + R1 * (mb + B * ma);
+  }
 };
 
 // Build the per-CTA tables: tw2 (and, for line passes, the gradient multipliers in register order).
@@ -147,6 +264,29 @@ __device__ __forceinline__ void build_tables(float2 *tw2, float2 *gp2, float2 *g
       gn2[q * RP + u] = gneg[k];
     }
   }
+}
+
+// Line-pass tables for an FFT policy F: twiddles, then the gradient multipliers i k e^{+-ikd/2}/N
+// in register order [idx][t] (pitch G+1).
+template <class F>
+__device__ __forceinline__ void build_line_tables(float2 *tw, float2 *gp2, float2 *gn2, const float2 *g,
+                                                  const float2 *gpos, const float2 *gneg) {
+  F::build_tw(tw, g);
+  constexpr int RP = F::G + 1;
+  for (int e = threadIdx.x; e < F::E * F::G; e += blockDim.x) {
+    const int q = e / F::G, u = e - q * F::G;
+    const int k = F::k_of(u, q);
+    gp2[q * RP + u] = gpos[k];
+    gn2[q * RP + u] = gneg[k];
+  }
+}
+template <class F>
+__host__ __device__ constexpr size_t pline_offset(int L) {
+  return (((size_t)L * F::LP + F::TW + 2 * (size_t)F::E * (F::G + 1)) * sizeof(float2) + 15) & ~size_t(15);
+}
+template <class F>
+__host__ __device__ constexpr size_t pline_smem(int L) {
+  return pline_offset<F>(L) + 2 * (size_t)(2 * L) * F::N * sizeof(float);
 }
 
 template <int E, int G>
@@ -177,16 +317,16 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // fused per-axis line pass (same algorithm as kwb::k_line_pass)
 // ------------------------------------------------------------------------------------------
 
-template <int E, int G, bool CONTIG, int LT>
-__global__ void __launch_bounds__(LT * G, E <= 16 ? 2 * (KWB_THREADS / (LT * G)) : 1)
+template <class F, bool CONTIG, int LT, int MINB>
+__global__ void __launch_bounds__(LT * F::G, MINB)
     k_line_fast(const SimDev *__restrict__ sims, int axis, int mode, long long step_s) {
-  using F = LineFFT<E, G, CONTIG>;
-  constexpr int RP = F::RP, LP = F::LP;
+  constexpr int E = F::E, G = F::G;
+  constexpr int RP = G + 1, LP = F::LP;
   constexpr int L = LT;  // complex lines per tile
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
-  float2 *gp2 = tw2 + E * RP;
+  float2 *gp2 = tw2 + F::TW;
   float2 *gn2 = gp2 + E * RP;
   const SimDev &S = sims[0];
   const long long t = *S.t0 + step_s;
@@ -246,7 +386,7 @@ __global__ void __launch_bounds__(LT * G, E <= 16 ? 2 * (KWB_THREADS / (LT * G))
   // asynchronous 16-byte copies: every load of the tile is in flight at once, overlapping the
   // table set-up and, for rho0, the first transform.  Staged layout: CONTIG [row][i],
   // strided [i][column] (the tile's own global layout, compacted).
-  float *st_p = reinterpret_cast<float *>(reinterpret_cast<char *>(smem_raw) + line_stage_offset<E, G>(L));
+  float *st_p = reinterpret_cast<float *>(reinterpret_cast<char *>(smem_raw) + pline_offset<F>(L));
   float *st_r = st_p + 2 * L * N;
   auto stage = [&](float *dst, const float *f) {
     const float *fb = f + base;
@@ -271,7 +411,7 @@ __global__ void __launch_bounds__(LT * G, E <= 16 ? 2 * (KWB_THREADS / (LT * G))
   stage(st_p, S.p);
   if (rho0) stage(st_r, rho0);
   else cp_async_commit();
-  build_tables<E, G>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
+  build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
   float2 *xs = sm + l * LP;
   float *__restrict__ ud = S.u[axis];
   // operand prefetch ahead of the transform arithmetic (dropped for E = 32 to stay in registers)
@@ -414,10 +554,10 @@ __global__ void __launch_bounds__(LT * G, E <= 16 ? 2 * (KWB_THREADS / (LT * G))
 // equation of state: x R2C, y/z C2C with the multiply innermost, x C2R
 // ------------------------------------------------------------------------------------------
 
-template <int E, int G, int LT>
-__global__ void __launch_bounds__(LT * G)
+template <class F, int LT, int MINB>
+__global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_fwd_fast(const SimDev *__restrict__ sims, long long step_s) {
-  using F = LineFFT<E, G, true>;
+  constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
@@ -432,7 +572,7 @@ __global__ void __launch_bounds__(LT * G)
   const int cnt = min(rows, Ny - y0);
   const long long base = ((long long)z * Ny + y0) * N;
   const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
-  build_tables<E, G>(tw2, nullptr, nullptr, S.tw[0], nullptr, nullptr);
+  F::build_tw(tw2, S.tw[0]);
   // One field at a time over all E positions: each loop issues 2E independent loads, so
   // every thread keeps many requests in flight (the sum, nonlinearity and c^2 follow).
   auto ld = [&](const float *__restrict__ f, int i) -> float2 {
@@ -475,7 +615,7 @@ __global__ void __launch_bounds__(LT * G)
   F::fwd(v, xs, tw2, tt);
 #pragma unroll
   for (int idx = 0; idx < E; ++idx) xs[F::k_of(tt, idx)] = v[idx];
-  __syncwarp();
+  F::sync();
   const int n1 = S.n1;
   const long long rowa = (long long)z * Ny + y0 + 2 * l;
   for (int k = tt; k < n1; k += G) {
@@ -486,10 +626,10 @@ __global__ void __launch_bounds__(LT * G)
   }
 }
 
-template <int E, int G, int LT>
-__global__ void __launch_bounds__(LT * G)
+template <class F, int LT, int MINB>
+__global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_inv_fast(const SimDev *__restrict__ sims, long long step_s) {
-  using F = LineFFT<E, G, true>;
+  constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
@@ -504,7 +644,7 @@ __global__ void __launch_bounds__(LT * G)
   const int cnt = min(rows, Ny - y0);
   const long long base = ((long long)z * Ny + y0) * N;
   const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
-  build_tables<E, G>(tw2, nullptr, nullptr, S.tw[0], nullptr, nullptr);
+  F::build_tw(tw2, S.tw[0]);
   float2 *xs = sm + l * LP;
   const int n1 = S.n1;
   const long long rowa = (long long)z * Ny + y0 + 2 * l;
@@ -543,7 +683,7 @@ __global__ void __launch_bounds__(LT * G)
       pn[PFS ? r : 0] = make_float2(va ? gd->pmin[ra + i] : 0.f, vb ? gd->pmin[rb + i] : 0.f);
     }
   }
-  __syncwarp();
+  F::sync();
   F::inv(v, xs, tw2, tt);
   float *__restrict__ p = S.p;
 #pragma unroll
@@ -574,10 +714,10 @@ __global__ void __launch_bounds__(LT * G)
   }
 }
 
-template <int E, int G, int LT>
-__global__ void __launch_bounds__(LT * G)
+template <class F, int LT, int MINB>
+__global__ void __launch_bounds__(LT * F::G, MINB)
     k_spec_fast(const SimDev *__restrict__ sims, int axis, int op, long long step_s) {
-  using F = LineFFT<E, G, false>;
+  constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
@@ -599,7 +739,7 @@ __global__ void __launch_bounds__(LT * G)
     base = (long long)o * n1 + k0 + l;
     stride = (long long)n1 * Ny;
   }
-  build_tables<E, G>(tw2, nullptr, nullptr, S.tw[axis], nullptr, nullptr);
+  F::build_tw(tw2, S.tw[axis]);
   float2 *xs = sm + l * LP;
   float2 *__restrict__ spec = S.spec;
   float2 v[E];
@@ -664,75 +804,170 @@ struct Tiles {
   static constexpr int SMALL = (32 / G > 2 ? 32 / G : 2);
 };
 
-template <int E, int G, int LT>
-static cudaError_t prime_lt() {
-  cudaError_t e;
-  const size_t ln = line_smem<E, G>(LT), lst = line_smem_staged<E, G>(LT);
-  if ((e = raise_smem((const void *)k_line_fast<E, G, true, LT>, lst)) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_line_fast<E, G, false, LT>, lst)) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_eos_fwd_fast<E, G, LT>, ln)) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_eos_inv_fast<E, G, LT>, ln)) != cudaSuccess) return e;
-  return raise_smem((const void *)k_spec_fast<E, G, LT>, ln);
-}
-
-template <int E, int G>
-static cudaError_t prime_size() {
-  cudaError_t e = prime_lt<E, G, Tiles<G>::BIG>();
-  if (e != cudaSuccess) return e;
-  return prime_lt<E, G, Tiles<G>::SMALL>();
-}
-
 static bool want_small(const SimDev &h, long long tiles_big) {
   return tiles_big < 2LL * (h.num_sms > 0 ? h.num_sms : 148);
 }
 
-template <int E, int G, int LT>
+// Tile variant per pass: 0 = big (THREADS per CTA), 1 = mid (128 threads), 2 = small (one warp).
+static int tile_variant(const SimDev &h, long long tiles_big) {
+  if (h.tile_override >= 0) return h.tile_override;
+  return want_small(h, tiles_big) ? 2 : 0;
+}
+
+// Line-pass configurations: FFT policy, threads per CTA and CTAs per SM to target.  The
+// three-level policy (8 registers-worth of elements per thread) is used for 128..1024, the
+// two-level one for 64.
+template <int N>
+struct LinePolicy;
+template <>
+struct LinePolicy<64> {
+  template <bool C> using F = LineFFT<8, 8, C>;
+  static constexpr int THREADS = 256, MINB = 2;
+};
+template <>
+struct LinePolicy<128> {
+  template <bool C> using F = LineFFT3<8, 2, 8, C>;
+  static constexpr int THREADS = 512, MINB = 2;
+};
+template <>
+struct LinePolicy<256> {
+  template <bool C> using F = LineFFT3<8, 4, 8, C>;
+  static constexpr int THREADS = 512, MINB = 2;
+};
+template <>
+struct LinePolicy<512> {
+  template <bool C> using F = LineFFT3<8, 8, 8, false>;  // 64 threads per line: block-level sync
+  static constexpr int THREADS = 512, MINB = 2;
+};
+template <>
+struct LinePolicy<1024> {
+  template <bool C> using F = LineFFT3<16, 8, 8, false>;
+  static constexpr int THREADS = 512, MINB = 1;
+};
+
+template <int N, bool C, int LT>
+static cudaError_t prime_line_variant() {
+  using P = LinePolicy<N>;
+  using F = typename P::template F<C>;
+  return raise_smem((const void *)k_line_fast<F, C, LT, P::MINB>, pline_smem<F>(LT));
+}
+
+template <int N>
+static cudaError_t prime_line() {
+  using P = LinePolicy<N>;
+  constexpr int G = P::template F<true>::G;
+  constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
+  cudaError_t e;
+  if ((e = prime_line_variant<N, true, BIG>()) != cudaSuccess) return e;
+  if ((e = prime_line_variant<N, false, BIG>()) != cudaSuccess) return e;
+  if ((e = prime_line_variant<N, true, SMALL>()) != cudaSuccess) return e;
+  if ((e = prime_line_variant<N, false, SMALL>()) != cudaSuccess) return e;
+  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  if ((e = prime_line_variant<N, true, MID>()) != cudaSuccess) return e;
+  return prime_line_variant<N, false, MID>();
+}
+
+template <int N, int LT>
 static void line_go(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s, cudaStream_t st) {
-  if (axis == 0)
-    k_line_fast<E, G, true, LT><<<cdiv(h.N[1], 2 * LT) * h.N[2], LT * G, line_smem_staged<E, G>(LT), st>>>(d_sim, axis, mode, s);
-  else
-    k_line_fast<E, G, false, LT><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * G,
-                                   line_smem_staged<E, G>(LT), st>>>(d_sim, axis, mode, s);
+  using P = LinePolicy<N>;
+  if (axis == 0) {
+    using F = typename P::template F<true>;
+    k_line_fast<F, true, LT, P::MINB><<<cdiv(h.N[1], 2 * LT) * h.N[2], LT * F::G, pline_smem<F>(LT), st>>>(
+        d_sim, axis, mode, s);
+  } else {
+    using F = typename P::template F<false>;
+    k_line_fast<F, false, LT, P::MINB><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G,
+                                         pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
+  }
 }
 
-template <int E, int G>
-static cudaError_t launch_line(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
-                               cudaStream_t st) {
-  constexpr int B = Tiles<G>::BIG;
-  const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * B) * h.N[2]
-                                    : (long long)cdiv(h.N[0], 2 * B) * (axis == 1 ? h.N[2] : h.N[1]);
-  if (want_small(h, tiles)) line_go<E, G, Tiles<G>::SMALL>(d_sim, h, axis, mode, s, st);
-  else line_go<E, G, B>(d_sim, h, axis, mode, s, st);
+template <int N>
+static cudaError_t launch_line_n(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                                 cudaStream_t st) {
+  using P = LinePolicy<N>;
+  constexpr int G = P::template F<true>::G;
+  constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
+  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * BIG) * h.N[2]
+                                    : (long long)cdiv(h.N[0], 2 * BIG) * (axis == 1 ? h.N[2] : h.N[1]);
+  switch (tile_variant(h, tiles)) {
+    case 1: line_go<N, MID>(d_sim, h, axis, mode, s, st); break;
+    case 2: line_go<N, SMALL>(d_sim, h, axis, mode, s, st); break;
+    default: line_go<N, BIG>(d_sim, h, axis, mode, s, st); break;
+  }
   return cudaGetLastError();
 }
 
-template <int E, int G, int LT>
+template <class F>
+__host__ __device__ constexpr size_t eos_smem(int L) {
+  return ((size_t)L * F::LP + F::TW) * sizeof(float2);
+}
+
+template <int N, int LT>
+static cudaError_t prime_eos_variant() {
+  using P = LinePolicy<N>;
+  using FC = typename P::template F<true>;
+  using FS = typename P::template F<false>;
+  cudaError_t e;
+  if ((e = raise_smem((const void *)k_eos_fwd_fast<FC, LT, P::MINB>, eos_smem<FC>(LT))) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_inv_fast<FC, LT, P::MINB>, eos_smem<FC>(LT))) != cudaSuccess) return e;
+  return raise_smem((const void *)k_spec_fast<FS, LT, P::MINB>, eos_smem<FS>(LT));
+}
+
+template <int N>
+static cudaError_t prime_eos_n() {
+  using P = LinePolicy<N>;
+  constexpr int G = P::template F<true>::G;
+  constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
+  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  cudaError_t e = prime_eos_variant<N, BIG>();
+  if (e == cudaSuccess) e = prime_eos_variant<N, MID>();
+  return e != cudaSuccess ? e : prime_eos_variant<N, SMALL>();
+}
+
+template <int N, int LT>
 static void eos_go(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
+  using P = LinePolicy<N>;
+  using F = typename P::template F<true>;
   const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
-  if (fwd) k_eos_fwd_fast<E, G, LT><<<grid, LT * G, line_smem<E, G>(LT), st>>>(d_sim, s);
-  else k_eos_inv_fast<E, G, LT><<<grid, LT * G, line_smem<E, G>(LT), st>>>(d_sim, s);
+  if (fwd) k_eos_fwd_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+  else k_eos_inv_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
 }
 
-template <int E, int G>
-static cudaError_t launch_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
-  constexpr int B = Tiles<G>::BIG;
-  if (want_small(h, (long long)cdiv(h.N[1], 2 * B) * h.N[2])) eos_go<E, G, Tiles<G>::SMALL>(d_sim, h, fwd, s, st);
-  else eos_go<E, G, B>(d_sim, h, fwd, s, st);
+template <int N>
+static cudaError_t launch_eos_n(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
+  using P = LinePolicy<N>;
+  constexpr int G = P::template F<true>::G;
+  constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
+  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  switch (tile_variant(h, (long long)cdiv(h.N[1], 2 * BIG) * h.N[2])) {
+    case 1: eos_go<N, MID>(d_sim, h, fwd, s, st); break;
+    case 2: eos_go<N, SMALL>(d_sim, h, fwd, s, st); break;
+    default: eos_go<N, BIG>(d_sim, h, fwd, s, st); break;
+  }
   return cudaGetLastError();
 }
 
-template <int E, int G, int LT>
+template <int N, int LT>
 static void spec_go(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s, cudaStream_t st) {
+  using P = LinePolicy<N>;
+  using F = typename P::template F<false>;
   const int grid = cdiv(h.n1, LT) * (axis == 1 ? h.N[2] : h.N[1]);
-  k_spec_fast<E, G, LT><<<grid, LT * G, line_smem<E, G>(LT), st>>>(d_sim, axis, op, s);
+  k_spec_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, axis, op, s);
 }
 
-template <int E, int G>
-static cudaError_t launch_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
-                               cudaStream_t st) {
-  constexpr int B = Tiles<G>::BIG;
-  if (want_small(h, (long long)cdiv(h.n1, B) * (axis == 1 ? h.N[2] : h.N[1]))) spec_go<E, G, Tiles<G>::SMALL>(d_sim, h, axis, op, s, st);
-  else spec_go<E, G, B>(d_sim, h, axis, op, s, st);
+template <int N>
+static cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                                 cudaStream_t st) {
+  using P = LinePolicy<N>;
+  constexpr int G = P::template F<true>::G;
+  constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
+  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  switch (tile_variant(h, (long long)cdiv(h.n1, BIG) * (axis == 1 ? h.N[2] : h.N[1]))) {
+    case 1: spec_go<N, MID>(d_sim, h, axis, op, s, st); break;
+    case 2: spec_go<N, SMALL>(d_sim, h, axis, op, s, st); break;
+    default: spec_go<N, BIG>(d_sim, h, axis, op, s, st); break;
+  }
   return cudaGetLastError();
 }
 
@@ -750,16 +985,31 @@ bool fast_size(int N) { return N == 64 || N == 128 || N == 256 || N == 512 || N 
     default: return cudaErrorInvalidValue;                             \
   }
 
-cudaError_t fast_prime(int N) { KWB_FAST_SWITCH(N, prime_size, ()) }
+#define KWB_LINE_SWITCH(N, FN, ARGS)       \
+  switch (N) {                             \
+    case 64: return fast::FN<64> ARGS;     \
+    case 128: return fast::FN<128> ARGS;   \
+    case 256: return fast::FN<256> ARGS;   \
+    case 512: return fast::FN<512> ARGS;   \
+    case 1024: return fast::FN<1024> ARGS; \
+    default: return cudaErrorInvalidValue; \
+  }
+
+static cudaError_t prime_eos(int N) { KWB_LINE_SWITCH(N, prime_eos_n, ()) }
+static cudaError_t prime_line(int N) { KWB_LINE_SWITCH(N, prime_line, ()) }
+cudaError_t fast_prime(int N) {
+  cudaError_t e = prime_eos(N);
+  return e != cudaSuccess ? e : prime_line(N);
+}
 cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
                            cudaStream_t st) {
-  KWB_FAST_SWITCH(h.N[axis], launch_line, (d_sim, h, axis, mode, s, st))
+  KWB_LINE_SWITCH(h.N[axis], launch_line_n, (d_sim, h, axis, mode, s, st))
 }
 cudaError_t fast_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
-  KWB_FAST_SWITCH(h.N[0], launch_eos, (d_sim, h, fwd, s, st))
+  KWB_LINE_SWITCH(h.N[0], launch_eos_n, (d_sim, h, fwd, s, st))
 }
 cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s, cudaStream_t st) {
-  KWB_FAST_SWITCH(h.N[axis], launch_spec, (d_sim, h, axis, op, s, st))
+  KWB_LINE_SWITCH(h.N[axis], launch_spec_n, (d_sim, h, axis, op, s, st))
 }
 
 }  // namespace kwb

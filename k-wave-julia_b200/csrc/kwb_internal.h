@@ -107,7 +107,8 @@ struct SimDev {
   // pass as it writes p (no separate gather); nullptr when there is none.
   const struct GroupDev *dense_p;
 
-  int num_sms;  // multiprocessors of the device (tile sizing)
+  int num_sms;        // multiprocessors of the device (tile sizing)
+  int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
 };
 
 // Sensor group on the device.
