@@ -332,6 +332,8 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
   if ((e = launch_eos_x_fwd(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
   if (h.ndim == 2) {
     if ((e = launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, step_s, st)) != cudaSuccess) return e;
+  } else if (h.ndim == 3 && h.plane) {
+    if ((e = fast_plane(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
   } else if (h.ndim == 3) {
     if ((e = launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD, step_s, st)) != cudaSuccess) return e;
     if ((e = launch_spec_pass(S->d_sim, h, 2, KWB_SPEC_FWD_MUL_INV, step_s, st)) != cudaSuccess) return e;
@@ -346,7 +348,7 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
 }
 
 int count_launches(const kwb_sim *S) {
-  int n = (S->tr ? 1 : 0) + S->h.ndim + 2 + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? 3 : 0));
+  int n = (S->tr ? 1 : 0) + S->h.ndim + 2 + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? (S->h.plane ? 1 : 3) : 0));
   for (auto &g : S->groups)
     if (!g.spec.cartesian && g.n > 0 && !g.fused) ++n;
   return n;
@@ -445,6 +447,26 @@ int kwb_query_outputs(kwb_ctx *ctx, const kwb_problem *P, kwb_group_sizes *sizes
   for (int a = 0; a < P->ndim; ++a) nvox *= P->N[a];
   for (int g = 0; g < P->n_groups; ++g) group_sizes(P, P->groups[g], nvox, sizes[g]);
   if (p_final_full_len) *p_final_full_len = P->tr.data ? nvox : 0;
+  return KWB_OK;
+}
+
+// Capture KWB_CHUNK_STEPS steps (plus the device step-counter advance) as one CUDA graph that
+// is replayed for every full chunk.
+static int build_chunk_graph(kwb_sim *S) {
+  kwb_ctx *ctx = S->ctx;
+  const int K = KWB_CHUNK_STEPS;
+  cudaGraph_t g;
+  CU(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int s = 0; s < K && e == cudaSuccess; ++s) e = enqueue_step(S, s);
+  if (e == cudaSuccess) e = launch_advance_t0(S->d_t0, K, S->stream);
+  cudaError_t e2 = cudaStreamEndCapture(S->stream, &g);
+  if (e != cudaSuccess) return set_err(ctx, KWB_E_DEVICE, "graph capture: %s", cudaGetErrorString(e));
+  CU(e2);
+  e = cudaGraphInstantiate(&S->graph, g, 0);
+  cudaGraphDestroy(g);
+  CU(e);
+  S->graph_K = K;
   return KWB_OK;
 }
 
@@ -621,12 +643,25 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     h.pml_sg_def[a] = psd;
   }
   {
+    // 3-D y/z transforms in one cluster pass per kx plane (KWB_PLANE=0 keeps separate passes)
+    const char *pv = getenv("KWB_PLANE");
+    h.plane = (h.fast & 2) && D == 3 && !h.dispersion && fast_size(h.N[0]) && fast_plane_size(h.N[1], h.N[2]) &&
+              !(pv && strcmp(pv, "0") == 0) && fast_plane_available();
+  }
+  {
     float *Mt, *M2 = nullptr;
     CU(M.alloc(&Mt, h.nspec));
     if (h.dispersion) CU(M.alloc(&M2, h.nspec));
+    int *slot_ky = nullptr;
+    if (h.plane) {
+      std::vector<int> ky(h.N[1]);
+      fast_plane_slot_ky(h.N[1], ky.data());
+      CU(M.alloc(&slot_ky, h.N[1]));
+      if ((rc = upload(ctx, slot_ky, ky.data(), ky.size() * sizeof(int), st))) return rc;
+    }
     const double d3[3] = {P->d[0], D > 1 ? P->d[1] : 1.0, D > 2 ? P->d[2] : 1.0};
     CU(build_eos_multiplier(Mt, M2, h.N, d3, c_ref, P->dt, c_arr ? 1.0 : c_s * c_s, absorbing, tau,
-                            eta, y, st));
+                            eta, y, slot_ky, st));
     h.M = Mt;
     h.M2 = M2;
   }
@@ -834,20 +869,9 @@ static int sim_enqueue(kwb_sim *S, long long steps) {
     }
     return KWB_OK;
   }
-  const int K = 32;
-  if (steps >= K && !S->graph) {
-    cudaGraph_t g;
-    CU(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
-    for (int s = 0; s < K && e == cudaSuccess; ++s) e = enqueue_step(S, s);
-    if (e == cudaSuccess) e = launch_advance_t0(S->d_t0, K, S->stream);
-    cudaError_t e2 = cudaStreamEndCapture(S->stream, &g);
-    if (e != cudaSuccess) return set_err(ctx, KWB_E_DEVICE, "graph capture: %s", cudaGetErrorString(e));
-    CU(e2);
-    e = cudaGraphInstantiate(&S->graph, g, 0);
-    cudaGraphDestroy(g);
-    CU(e);
-    S->graph_K = K;
+  if (steps >= KWB_CHUNK_STEPS && !S->graph) {
+    const int rc = build_chunk_graph(S);
+    if (rc) return rc;
   }
   while (S->graph && steps >= S->graph_K) {
     CU(cudaGraphLaunch(S->graph, S->stream));
@@ -871,6 +895,11 @@ int kwb_sim_advance_timed(kwb_sim *S, int64_t steps, double *device_ms) {
   if (!S) return KWB_E_INVALID;
   kwb_ctx *ctx = S->ctx;
   CU(cudaSetDevice(ctx->device));
+  // capture the replayed chunk first, so that the timed interval holds device work only
+  if (!S->progress && !S->graph && steps >= KWB_CHUNK_STEPS && S->Nt_loop - S->steps_done >= KWB_CHUNK_STEPS) {
+    const int rc = build_chunk_graph(S);
+    if (rc) return rc;
+  }
   CU(cudaEventRecord(S->ev0, S->stream));
   int rc = sim_enqueue(S, steps);
   if (rc) return rc;
@@ -1061,6 +1090,8 @@ int kwb_sim_profile(kwb_sim *S, int64_t steps, kwb_kernel_times *out) {
     if (h.ndim == 2) {
       timed(slot("spec_y_mul", ns * 8.0 * (h.dispersion ? 3 : 2) + ns * 4.0 * (h.dispersion ? 2 : 1)),
             [&] { return launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, s, st); });
+    } else if (h.ndim == 3 && h.plane) {
+      timed(slot("spec_yz_plane", ns * 16.0 + ns * 4.0), [&] { return fast_plane(S->d_sim, h, s, st); });
     } else if (h.ndim == 3) {
       timed(slot("spec_y_fwd", ns * 16.0 * (h.dispersion ? 2 : 1)), [&] { return launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD, s, st); });
       timed(slot("spec_z_mul", ns * 8.0 * (h.dispersion ? 3 : 2) + ns * 4.0 * (h.dispersion ? 2 : 1)),

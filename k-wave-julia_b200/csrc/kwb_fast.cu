@@ -131,7 +131,9 @@ struct LineFFT {
     sync();
   }
   // frequency index held in register idx by thread t
-  __device__ __forceinline__ static int k_of(int t, int idx) { return t * J + idx / G + E * (idx % G); }
+  __host__ __device__ __forceinline__ static int k_of(int t, int idx) { return t * J + idx / G + E * (idx % G); }
+  __device__ __forceinline__ static int nat(int k) { return k; }  // natural-order spectrum slot
+  __device__ __forceinline__ static int nat_of(int t, int idx) { return k_of(t, idx); }
   // per-CTA twiddle table: exp(-2 pi i t q/N) at [q*(G+1) + t]
   static constexpr int TW = E * RP;
   __device__ __forceinline__ static void build_tw(float2 *tw2, const float2 *tw) {
@@ -153,11 +155,37 @@ struct LineFFT3 {
   static constexpr int E = R1, G = A * B, N = R1 * A * B;
   static constexpr int P2 = R1 / B, P3 = R1 / A;  // (q1, a) and (q1, m_b) pairs per thread
   static_assert(R1 % A == 0 && R1 % B == 0, "A and B must divide R1");
-  static constexpr int RP = G + 1;                 // pitch of the [q1][t] layout
-  static constexpr int AP = A + 1;                 // pitch of the [q1][m_b][a] layout
-  static constexpr int S1 = R1 * RP, S2 = R1 * B * AP;
-  static constexpr int LP = (S1 > S2 ? S1 : S2) + 1;
+  static constexpr int RP = G + 1;                 // pitch of the level-1 twiddle table
+  static constexpr int AP = A + 1;                 // pitch of the level-2 twiddle table
+  // Exchange layouts.  Each is a sum of one term per index (affine in the parts), so every
+  // access is a per-thread base plus a compile-time offset, and the pads are chosen so that the
+  // exchanges of a line held by one warp (contiguous passes) hit distinct banks in every stage:
+  //   level 1  [q][u]          q * RP1 + u
+  //   level 2  [q1][m_b][a]    q1 * Q2 + beta2(m_b) + a
+  //   natural  k = q1 + R1 (m_b + B m_a)  ->  q1 + beta3(m_b) + m_a * ZS   (EOS pair split)
+  // A line occupies LP (odd) slots, so lines held by one warp in strided passes, which all use
+  // the same offset within their line, also hit distinct banks.
+  static constexpr int PI = R1 == 16 ? 3 : A == 2 ? 0 : A == 4 ? 1 : 2;
+  static constexpr int RP1 = PI == 3 ? 65 : G + A;
+  static constexpr int M2 = PI == 0 ? 2 : PI == 1 ? 4 : PI == 2 ? 9 : 8, X2 = PI == 1 || PI == 3 ? 1 : 0;
+  static constexpr int Z2 = PI == 0 ? 1 : 0, Q2 = PI == 0 ? 18 : PI == 1 ? 36 : PI == 2 ? 72 : 68;
+  static constexpr int M3 = PI == 3 ? 16 : 8, X3 = PI == 2 ? 2 : 4, ZS = PI == 3 ? 140 : PI == 2 ? 70 : 76;
+  __host__ __device__ static constexpr int beta2(int mb) { return mb * M2 + (mb >> 1) * X2 + (mb >> 2) * Z2; }
+  __host__ __device__ static constexpr int beta3(int mb) { return mb * M3 + (mb >> 1) * X3; }
+  static constexpr int S1 = (R1 - 1) * RP1 + G, S2 = (R1 - 1) * Q2 + beta2(B - 1) + A;
+  static constexpr int S3 = R1 + beta3(B - 1) + (A - 1) * ZS;
+  static constexpr int SM = S1 > S2 ? (S1 > S3 ? S1 : S3) : (S2 > S3 ? S2 : S3);
+  static constexpr int LP = SM | 1;
   static constexpr int TW = R1 * RP + B * AP;      // level-1 then level-2 twiddles
+  __device__ __forceinline__ static int i1(int q, int u) { return q * RP1 + u; }
+  __device__ __forceinline__ static int i2(int q1, int mb, int a) { return q1 * Q2 + beta2(mb) + a; }
+  __device__ __forceinline__ static int nat3(int q1, int mb, int ma) { return q1 + beta3(mb) + ma * ZS; }
+  __device__ __forceinline__ static int nat(int k) { return nat3(k % R1, (k / R1) % B, k / (R1 * B)); }
+  // slot of register idx of thread t (the k_of position) in the natural-order layout
+  __device__ __forceinline__ static int nat_of(int t, int idx) {
+    const int p0 = t * P3, q1 = p0 / B, mb = p0 - q1 * B + idx / A;  // B is a multiple of P3
+    return nat3(q1, mb, idx % A);
+  }
   __device__ __forceinline__ static void sync() {
     if (WARP) __syncwarp();
     else __syncthreads();
@@ -176,14 +204,14 @@ struct LineFFT3 {
   __device__ __forceinline__ static void fwd(float2 (&v)[E], float2 *xs, const float2 *tw, int t) {
     dft_reg<R1, false>(v);
 #pragma unroll
-    for (int q = 0; q < R1; ++q) xs[q * RP + t] = cmul(v[q], tw[q * RP + t]);
+    for (int q = 0; q < R1; ++q) xs[i1(q, t)] = cmul(v[q], tw[q * RP + t]);
     sync();
 #pragma unroll
     for (int j = 0; j < P2; ++j) {
       const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
       float2 w[B];
 #pragma unroll
-      for (int b = 0; b < B; ++b) w[b] = xs[q1 * RP + a + A * b];
+      for (int b = 0; b < B; ++b) w[b] = xs[i1(q1, a + A * b)];
       dft_reg<B, false>(w);
 #pragma unroll
       for (int mb = 0; mb < B; ++mb) v[j * B + mb] = cmul(w[mb], tw[R1 * RP + mb * AP + a]);
@@ -193,7 +221,7 @@ struct LineFFT3 {
     for (int j = 0; j < P2; ++j) {
       const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
 #pragma unroll
-      for (int mb = 0; mb < B; ++mb) xs[(q1 * B + mb) * AP + a] = v[j * B + mb];
+      for (int mb = 0; mb < B; ++mb) xs[i2(q1, mb, a)] = v[j * B + mb];
     }
     sync();
 #pragma unroll
@@ -201,7 +229,7 @@ struct LineFFT3 {
       const int p = t * P3 + j, q1 = p / B, mb = p - q1 * B;
       float2 w[A];
 #pragma unroll
-      for (int a = 0; a < A; ++a) w[a] = xs[(q1 * B + mb) * AP + a];
+      for (int a = 0; a < A; ++a) w[a] = xs[i2(q1, mb, a)];
       dft_reg<A, false>(w);
 #pragma unroll
       for (int ma = 0; ma < A; ++ma) v[j * A + ma] = w[ma];
@@ -218,7 +246,7 @@ struct LineFFT3 {
       for (int ma = 0; ma < A; ++ma) w[ma] = v[j * A + ma];
       dft_reg<A, true>(w);
 #pragma unroll
-      for (int a = 0; a < A; ++a) xs[(q1 * B + mb) * AP + a] = w[a];
+      for (int a = 0; a < A; ++a) xs[i2(q1, mb, a)] = w[a];
     }
     sync();
 #pragma unroll
@@ -226,7 +254,7 @@ struct LineFFT3 {
       const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
       float2 w[B];
 #pragma unroll
-      for (int mb = 0; mb < B; ++mb) w[mb] = cmul_conj(xs[(q1 * B + mb) * AP + a], tw[R1 * RP + mb * AP + a]);
+      for (int mb = 0; mb < B; ++mb) w[mb] = cmul_conj(xs[i2(q1, mb, a)], tw[R1 * RP + mb * AP + a]);
       dft_reg<B, true>(w);
 #pragma unroll
       for (int b = 0; b < B; ++b) v[j * B + b] = w[b];
@@ -236,15 +264,15 @@ struct LineFFT3 {
     for (int j = 0; j < P2; ++j) {
       const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
 #pragma unroll
-      for (int b = 0; b < B; ++b) xs[q1 * RP + a + A * b] = v[j * B + b];
+      for (int b = 0; b < B; ++b) xs[i1(q1, a + A * b)] = v[j * B + b];
     }
     sync();
 #pragma unroll
-    for (int q = 0; q < R1; ++q) v[q] = cmul_conj(xs[q * RP + t], tw[q * RP + t]);
+    for (int q = 0; q < R1; ++q) v[q] = cmul_conj(xs[i1(q, t)], tw[q * RP + t]);
     dft_reg<R1, true>(v);
     sync();
   }
-  __device__ __forceinline__ static int k_of(int t, int idx) {
+  __host__ __device__ __forceinline__ static int k_of(int t, int idx) {
     const int p = t * P3 + idx / A, q1 = p / B, mb = p - q1 * B, ma = idx % A;
     return q1 + R1 * (mb + B * ma);
   }
@@ -414,8 +442,9 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
   float2 *xs = sm + l * LP;
   float *__restrict__ ud = S.u[axis];
-  // operand prefetch ahead of the transform arithmetic (dropped for E = 32 to stay in registers)
-  constexpr bool PF = E <= 16;
+  // velocity prefetch ahead of the transform arithmetic (contiguous tiles; strided tiles load
+  // it where it is used, to stay within 64 registers)
+  constexpr bool PF = CONTIG && E <= 16;
   float2 uu[PF ? E : 1];
   if (PF && mode == KWB_MODE_STEP) {
 #pragma unroll
@@ -433,7 +462,9 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gp2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
   cp_async_wait<0>();
-  __syncthreads();  // the rho0 tile has landed
+  __syncthreads();  // the rho0 tile has landed; every thread is done with the p tile
+  // the split density rho_d goes into the p tile's slot while d/dx_d u is transformed
+  if (mode == KWB_MODE_STEP) stage(st_p, S.rho[axis]);
 
   // velocity update u = pml_sg (pml_sg u - dt/rho_sg dp)
   const float *__restrict__ esg = S.pml_sg_def[axis];
@@ -444,7 +475,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     float2 coef;
     if (rho0) {
       const float2 r0 = staged(st_r, i), r1 = staged(st_r, inext);
-      coef = make_float2(S.dt / (0.5f * (r0.x + r1.x)), S.dt / (0.5f * (r0.y + r1.y)));
+      coef = make_float2(__fdividef(2.0f * S.dt, r0.x + r1.x), __fdividef(2.0f * S.dt, r0.y + r1.y));
     } else {
       coef = make_float2(S.dt_over_rho0_s, S.dt_over_rho0_s);
     }
@@ -496,12 +527,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     }
   }
   float *__restrict__ rd = S.rho[axis];
-  float2 rr[PF ? E : 1];
 #pragma unroll
-  for (int r = 0; r < E; ++r) {
-    store_pair(ud, tt + G * r, v[r]);
-    if (PF) rr[PF ? r : 0] = load_pair(rd, tt + G * r);
-  }
+  for (int r = 0; r < E; ++r) store_pair(ud, tt + G * r, v[r]);
 
   // d/dx_d u_d  (staggered -)
   F::fwd(v, xs, tw2, tt);
@@ -509,6 +536,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gn2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
 
+  cp_async_wait<0>();
+  __syncthreads();  // the rho_d tile has landed
   // density update rho_d = pml (pml rho_d - dt rho0 du)
   const float *__restrict__ ed = S.pml_def[axis];
 #pragma unroll
@@ -522,7 +551,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     } else {
       coef = make_float2(S.dt_rho0_s, S.dt_rho0_s);
     }
-    const float2 r0d = PF ? rr[PF ? r : 0] : load_pair(rd, i);
+    const float2 r0d = staged(st_p, i);
     float ta = fmaf(-ei, r0d.x, r0d.x), tb = fmaf(-ei, r0d.y, r0d.y);
     ta = fmaf(-coef.x, v[r].x, ta);
     tb = fmaf(-coef.y, v[r].y, tb);
@@ -554,7 +583,9 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 // equation of state: x R2C, y/z C2C with the multiply innermost, x C2R
 // ------------------------------------------------------------------------------------------
 
-template <class F, int LT, int MINB>
+// PLANE: write the half spectrum as [z][kx][y] (rows of y for the cluster y-z pass), instead of
+// [z][y][kx].
+template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_fwd_fast(const SimDev *__restrict__ sims, long long step_s) {
   constexpr int E = F::E, G = F::G;
@@ -614,19 +645,36 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   float2 *xs = sm + l * LP;
   F::fwd(v, xs, tw2, tt);
 #pragma unroll
-  for (int idx = 0; idx < E; ++idx) xs[F::k_of(tt, idx)] = v[idx];
-  F::sync();
+  for (int idx = 0; idx < E; ++idx) xs[F::nat_of(tt, idx)] = v[idx];
   const int n1 = S.n1;
+  if (PLANE) {
+    // one (kx, line pair) per thread, pairs fastest: the pair's two rows are adjacent in y, so
+    // each thread writes A and B as one 16-byte store and each kx gets 2L consecutive y
+    __syncthreads();
+    for (int e = tid; e < n1 * L; e += blockDim.x) {
+      const int k = e / L, lp = e - k * L;
+      if (2 * lp >= cnt) continue;
+      const float2 *xl = sm + lp * LP;
+      const float2 zz = xl[F::nat(k)], zm = xl[F::nat(k == 0 ? 0 : N - k)];
+      float2 *dst = S.spec + ((long long)z * n1 + k) * Ny + y0 + 2 * lp;
+      const float2 A = make_float2(0.5f * (zz.x + zm.x), 0.5f * (zz.y - zm.y));
+      const float2 B = make_float2(0.5f * (zz.y + zm.y), -0.5f * (zz.x - zm.x));
+      if (2 * lp + 1 < cnt) *reinterpret_cast<float4 *>(dst) = make_float4(A.x, A.y, B.x, B.y);
+      else *dst = A;
+    }
+    return;
+  }
+  F::sync();
   const long long rowa = (long long)z * Ny + y0 + 2 * l;
   for (int k = tt; k < n1; k += G) {
-    const float2 zz = xs[k];
-    const float2 zm = xs[k == 0 ? 0 : N - k];
+    const float2 zz = xs[F::nat(k)];
+    const float2 zm = xs[F::nat(k == 0 ? 0 : N - k)];
     if (va) S.spec[rowa * n1 + k] = make_float2(0.5f * (zz.x + zm.x), 0.5f * (zz.y - zm.y));
     if (vb) S.spec[(rowa + 1) * n1 + k] = make_float2(0.5f * (zz.y + zm.y), -0.5f * (zz.x - zm.x));
   }
 }
 
-template <class F, int LT, int MINB>
+template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_inv_fast(const SimDev *__restrict__ sims, long long step_s) {
   constexpr int E = F::E, G = F::G;
@@ -647,21 +695,45 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   F::build_tw(tw2, S.tw[0]);
   float2 *xs = sm + l * LP;
   const int n1 = S.n1;
-  const long long rowa = (long long)z * Ny + y0 + 2 * l;
-  for (int k = tt; k < n1; k += G) {
-    const float2 A = va ? S.spec[rowa * n1 + k] : make_float2(0.f, 0.f);
-    const float2 B = vb ? S.spec[(rowa + 1) * n1 + k] : make_float2(0.f, 0.f);
-    if (k == 0 || 2 * k == N) {
-      xs[k] = make_float2(A.x, B.x);  // c2r ignores Im of the DC and Nyquist bins
-    } else {
-      xs[k] = make_float2(A.x - B.y, A.y + B.x);
-      xs[N - k] = make_float2(A.x + B.y, B.x - A.y);
+  if (PLANE) {
+    // one (kx, line pair) per thread, pairs fastest: the pair's rows are adjacent in y, so A and
+    // B arrive as one 16-byte load and each kx reads 2L consecutive y
+    for (int e = tid; e < n1 * L; e += blockDim.x) {
+      const int k = e / L, lp = e - k * L;
+      const float2 *srcp = S.spec + ((long long)z * n1 + k) * Ny + y0 + 2 * lp;
+      float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+      if (2 * lp + 1 < cnt) {
+        const float4 ab = *reinterpret_cast<const float4 *>(srcp);
+        A = make_float2(ab.x, ab.y);
+        B = make_float2(ab.z, ab.w);
+      } else if (2 * lp < cnt) {
+        A = *srcp;
+      }
+      float2 *xl = sm + lp * LP;
+      if (k == 0 || 2 * k == N) {
+        xl[F::nat(k)] = make_float2(A.x, B.x);  // c2r ignores Im of the DC and Nyquist bins
+      } else {
+        xl[F::nat(k)] = make_float2(A.x - B.y, A.y + B.x);
+        xl[F::nat(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+      }
+    }
+  } else {
+    const long long rowa = (long long)z * Ny + y0 + 2 * l;
+    for (int k = tt; k < n1; k += G) {
+      const float2 A = va ? S.spec[rowa * n1 + k] : make_float2(0.f, 0.f);
+      const float2 B = vb ? S.spec[(rowa + 1) * n1 + k] : make_float2(0.f, 0.f);
+      if (k == 0 || 2 * k == N) {
+        xs[F::nat(k)] = make_float2(A.x, B.x);  // c2r ignores Im of the DC and Nyquist bins
+      } else {
+        xs[F::nat(k)] = make_float2(A.x - B.y, A.y + B.x);
+        xs[F::nat(N - k)] = make_float2(A.x + B.y, B.x - A.y);
+      }
     }
   }
   __syncthreads();
   float2 v[E];
 #pragma unroll
-  for (int idx = 0; idx < E; ++idx) v[idx] = xs[F::k_of(tt, idx)];
+  for (int idx = 0; idx < E; ++idx) v[idx] = xs[F::nat_of(tt, idx)];
   // dense pressure sensor (record_sensor_data!, first_order_steps.jl:732-752): prefetch the
   // running max/min before the transform, update all fields as p is written
   const GroupDev *gd = S.dense_p;
@@ -776,6 +848,145 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   if (valid) {
 #pragma unroll
     for (int r = 0; r < E; ++r) spec[base + (long long)(tt + G * r) * stride] = v[r];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// y and z transforms of the equation of state, one kx plane per thread-block cluster
+// ------------------------------------------------------------------------------------------
+
+#define KWB_PLANE_THREADS 512
+
+// Distributed shared memory: 32-bit shared::cluster addresses of the same offset in another CTA.
+__device__ __forceinline__ unsigned cta_smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned cluster_map(unsigned addr, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ float2 cluster_ld(unsigned addr) {
+  float2 v;
+  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void cluster_st(unsigned addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};\n" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+
+// Plane pass: the spectrum is [z][kx][y] (k_eos_fwd_fast<PLANE>), so plane kx is NZ rows of NY
+// contiguous values.  The CL CTAs of a cluster share plane kx: CTA r holds z rows
+// [r RZ, (r+1) RZ) in shared memory and
+//   1. transforms its rows along y (contiguous lines, one warp per line) and keeps each row in
+//      register order: slot s = t + G idx holds k_y = FY::k_of(t, idx);
+//   2. after a cluster barrier, transforms along z the slots [r CY, (r+1) CY) of every row of
+//      the plane (lines spread over the warps as in the strided line passes, so that a warp's
+//      loads cover consecutive slots of one row), loading element z of a slot from the CTA that
+//      holds row z (distributed shared memory), multiplies by M[kx][k_z][slot] and transforms
+//      back, storing each element to the CTA it came from;
+//   3. after a second barrier, transforms its rows back along y and writes them to the plane.
+// The spectrum crosses HBM once in and once out per step, with the multiplier read once.
+template <class FY, class FZ, int CL>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 2)
+    k_plane_fast(const SimDev *__restrict__ sims, long long step_s) {
+  constexpr int NY = FY::N, NZ = FZ::N, RZ = NZ / CL, CY = NY / CL;
+  constexpr int LY = KWB_PLANE_THREADS / FY::G, LZ = KWB_PLANE_THREADS / FZ::G;
+  static_assert(RZ == 2 * LY && CY % LZ == 0 && RZ == FZ::G, "plane tiling");
+  constexpr int XS = (LY * FY::LP > LZ * FZ::LP) ? LY * FY::LP : LZ * FZ::LP;
+  extern __shared__ float4 smem_raw[];
+  float2 *data = reinterpret_cast<float2 *>(smem_raw);  // [RZ][NY]
+  float2 *xsb = data + RZ * NY;
+  float2 *twy = xsb + XS;
+  float2 *twz = twy + FY::TW;
+  const SimDev &S = sims[0];
+  const long long t = *S.t0 + step_s;
+  if (t >= S.Nt) return;  // uniform over the cluster
+  const unsigned rank = cluster_rank();
+  const int kx = blockIdx.x / CL;
+  const int tid = threadIdx.x;
+  const long long rstride = (long long)S.n1 * NY;  // between consecutive z rows of the plane
+  float2 *plane = S.spec + (long long)rank * RZ * rstride + (long long)kx * NY;
+  // rows in two groups, so that the first transforms start while the second group lands
+  constexpr int CPR = NY / 2;  // 16-byte chunks per row
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    for (int q = tid; q < LY * CPR; q += KWB_PLANE_THREADS) {
+      const int r = g * LY + q / CPR, c = q % CPR;
+      cp_async16(data + r * NY + 2 * c, plane + r * rstride + 2 * c, 16);
+    }
+    cp_async_commit();
+  }
+  FY::build_tw(twy, S.tw[1]);
+  FZ::build_tw(twz, S.tw[2]);
+
+  // 1. forward along y
+  {
+    const int tt = tid % FY::G, l = tid / FY::G;
+    float2 *xs = xsb + l * FY::LP;
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      if (g == 0) cp_async_wait<1>();
+      else cp_async_wait<0>();
+      __syncthreads();
+      float2 *row = data + (g * LY + l) * NY;
+      float2 v[FY::E];
+#pragma unroll
+      for (int r = 0; r < FY::E; ++r) v[r] = row[tt + FY::G * r];
+      FY::fwd(v, xs, twy, tt);
+#pragma unroll
+      for (int idx = 0; idx < FY::E; ++idx) row[tt + FY::G * idx] = v[idx];
+    }
+  }
+  cluster_barrier();
+
+  // 2. along z, multiply, back along z
+  {
+    const int l = tid % LZ, tt = tid / LZ;
+    float2 *xs = xsb + l * FZ::LP;
+    const float *__restrict__ Mp = S.M + (long long)kx * NZ * NY;
+#pragma unroll 1
+    for (int c0 = 0; c0 < CY; c0 += LZ) {
+      const int sl = (int)rank * CY + c0 + l;  // slot (register-order k_y) of this line
+      float m[FZ::E];
+#pragma unroll
+      for (int idx = 0; idx < FZ::E; ++idx) m[idx] = __ldg(Mp + (long long)FZ::k_of(tt, idx) * NY + sl);
+      // element z = tt + G r is row tt of CTA r (RZ == G)
+      const unsigned a0 = cta_smem_addr(data + tt * NY + sl);
+      float2 v[FZ::E];
+#pragma unroll
+      for (int r = 0; r < FZ::E; ++r) v[r] = cluster_ld(cluster_map(a0, (unsigned)r));
+      FZ::fwd(v, xs, twz, tt);
+#pragma unroll
+      for (int idx = 0; idx < FZ::E; ++idx) v[idx] = make_float2(v[idx].x * m[idx], v[idx].y * m[idx]);
+      FZ::inv(v, xs, twz, tt);
+#pragma unroll
+      for (int r = 0; r < FZ::E; ++r) cluster_st(cluster_map(a0, (unsigned)r), v[r]);
+    }
+  }
+  cluster_barrier();
+
+  // 3. back along y, straight to the plane
+  {
+    const int tt = tid % FY::G, l = tid / FY::G;
+    float2 *xs = xsb + l * FY::LP;
+#pragma unroll 1
+    for (int g = 0; g < 2; ++g) {
+      const float2 *row = data + (g * LY + l) * NY;
+      float2 v[FY::E];
+#pragma unroll
+      for (int idx = 0; idx < FY::E; ++idx) v[idx] = row[tt + FY::G * idx];
+      FY::inv(v, xs, twy, tt);
+      float2 *out = plane + (g * LY + l) * rstride;
+#pragma unroll
+      for (int r = 0; r < FY::E; ++r) out[tt + FY::G * r] = v[r];
+    }
   }
 }
 
@@ -909,8 +1120,10 @@ static cudaError_t prime_eos_variant() {
   using FC = typename P::template F<true>;
   using FS = typename P::template F<false>;
   cudaError_t e;
-  if ((e = raise_smem((const void *)k_eos_fwd_fast<FC, LT, P::MINB>, eos_smem<FC>(LT))) != cudaSuccess) return e;
-  if ((e = raise_smem((const void *)k_eos_inv_fast<FC, LT, P::MINB>, eos_smem<FC>(LT))) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_fwd_fast<FC, LT, P::MINB, false>, eos_smem<FC>(LT))) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_inv_fast<FC, LT, P::MINB, false>, eos_smem<FC>(LT))) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_fwd_fast<FC, LT, P::MINB, true>, eos_smem<FC>(LT))) != cudaSuccess) return e;
+  if ((e = raise_smem((const void *)k_eos_inv_fast<FC, LT, P::MINB, true>, eos_smem<FC>(LT))) != cudaSuccess) return e;
   return raise_smem((const void *)k_spec_fast<FS, LT, P::MINB>, eos_smem<FS>(LT));
 }
 
@@ -930,8 +1143,13 @@ static void eos_go(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, 
   using P = LinePolicy<N>;
   using F = typename P::template F<true>;
   const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
-  if (fwd) k_eos_fwd_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
-  else k_eos_inv_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+  if (h.plane) {
+    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+    else k_eos_inv_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+  } else {
+    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+    else k_eos_inv_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+  }
 }
 
 template <int N>
@@ -971,7 +1189,54 @@ static cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, int axis,
   return cudaGetLastError();
 }
 
+// Cluster plane pass for Ny = Nz = 256: 8 CTAs of 512 threads per kx plane, 32 rows each.
+using PlaneFY = LinePolicy<256>::F<true>;
+using PlaneFZ = LinePolicy<256>::F<false>;
+constexpr int kPlaneCL = 8;
+constexpr size_t plane_smem() {
+  constexpr int RZ = 256 / kPlaneCL, LY = KWB_PLANE_THREADS / PlaneFY::G, LZ = KWB_PLANE_THREADS / PlaneFZ::G;
+  constexpr int XS = (LY * PlaneFY::LP > LZ * PlaneFZ::LP) ? LY * PlaneFY::LP : LZ * PlaneFZ::LP;
+  return ((size_t)RZ * 256 + XS + PlaneFY::TW + PlaneFZ::TW) * sizeof(float2);
+}
+static int plane_clusters_per_device() {
+  const void *fn = (const void *)k_plane_fast<PlaneFY, PlaneFZ, kPlaneCL>;
+  if (raise_smem(fn, plane_smem()) != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kPlaneCL * 16);
+  cfg.blockDim = dim3(KWB_PLANE_THREADS);
+  cfg.dynamicSmemBytes = plane_smem();
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeClusterDimension;
+  at.val.clusterDim.x = kPlaneCL;
+  at.val.clusterDim.y = 1;
+  at.val.clusterDim.z = 1;
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
 }  // namespace fast
+
+bool fast_plane_size(int Ny, int Nz) { return Ny == 256 && Nz == 256; }
+bool fast_plane_available() {
+  static int n = -1;  // clusters that fit on the device at once (checked once per process)
+  if (n < 0) n = fast::plane_clusters_per_device();
+  return n > 0;
+}
+// Register-order slot -> k_y of the plane pass's y transform (the layout of its multiplier).
+void fast_plane_slot_ky(int Ny, int *ky) {
+  using F = fast::PlaneFY;
+  for (int s = 0; s < Ny; ++s) ky[s] = F::k_of(s % F::G, s / F::G);
+}
+cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
+  fast::k_plane_fast<fast::PlaneFY, fast::PlaneFZ, fast::kPlaneCL>
+      <<<h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st>>>(d_sim, s);
+  return cudaGetLastError();
+}
 
 bool fast_size(int N) { return N == 64 || N == 128 || N == 256 || N == 512 || N == 1024; }
 

@@ -16,6 +16,7 @@
 #define KWB_MAX_STAGES 16
 #define KWB_THREADS 256
 #define KWB_MAX_N 4096
+#define KWB_CHUNK_STEPS 32  // time steps per replayed CUDA graph
 
 struct FftPlan {
   int n;
@@ -102,6 +103,10 @@ struct SimDev {
   const long long *t0;  // device step base (CUDA graph replays advance it)
 
   int fast;  // register-FFT kernels (kwb_fast.cu) for power-of-two lines: bit 0 line passes, bit 1 EOS passes
+  // 3-D equation of state with the y/z transforms in one cluster pass per kx plane: the half
+  // spectrum is then [z][kx][y] and M is [kx][k_z][slot] (slot: register order of the pass's y
+  // transform, fast_plane_slot_ky)
+  int plane;
 
   // A dense (every-voxel) sensor group recording only pressure fields, updated by the x C2R
   // pass as it writes p (no separate gather); nullptr when there is none.
@@ -154,6 +159,10 @@ cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int m
 cudaError_t fast_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
 cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
                       cudaStream_t st);
+bool fast_plane_size(int Ny, int Nz);
+bool fast_plane_available();
+void fast_plane_slot_ky(int Ny, int *ky);
+cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
 
 // FP64 table builders.
 cudaError_t build_twiddles(float2 *out, int N, cudaStream_t st);
@@ -162,7 +171,8 @@ cudaError_t build_pml_deficit(float *out, int N, int pml_size, double alpha, dou
                               int staggered, cudaStream_t st);
 cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const double d[3],
                                  double c_ref, double dt, double c_sq_fold, int absorbing,
-                                 double tau, double eta, double y, cudaStream_t st);
+                                 double tau, double eta, double y, const int *slot_ky,
+                                 cudaStream_t st);
 cudaError_t convert_f64_to_f32(float *out, const double *in, long long n, int op,
                                cudaStream_t st);
 cudaError_t build_nlq(float *out, const double *bona, int bona_array, double bona_s,

@@ -53,17 +53,26 @@ __global__ void k_build_pml_deficit(float *out, int N, int pml_size, double alph
   }
 }
 
+// Layouts: [k_z][k_y][k_x] (slot_ky == nullptr) or, for the cluster plane pass,
+// [k_x][k_z][slot] with k_y = slot_ky[slot].
 __global__ void k_build_eos_multiplier(float *M, float *M2, int Nx, int Ny, int Nz, double dx,
                                        double dy, double dz, double c_ref, double dt,
                                        double c_sq_fold, int absorbing, double tau, double eta,
-                                       double y) {
+                                       double y, const int *slot_ky) {
   const int n1 = Nx / 2 + 1;
   const long long total = (long long)n1 * Ny * Nz;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= total) return;
-  const int kx = (int)(idx % n1);
-  const int ky = (int)((idx / n1) % Ny);
-  const int kz = (int)(idx / ((long long)n1 * Ny));
+  int kx, ky, kz;
+  if (slot_ky) {
+    ky = slot_ky[(int)(idx % Ny)];
+    kz = (int)((idx / Ny) % Nz);
+    kx = (int)(idx / ((long long)Ny * Nz));
+  } else {
+    kx = (int)(idx % n1);
+    ky = (int)((idx / n1) % Ny);
+    kz = (int)(idx / ((long long)n1 * Ny));
+  }
   const double a = wavenumber(kx, Nx, dx);
   const double b = Ny > 1 ? wavenumber(ky, Ny, dy) : 0.0;
   const double c = Nz > 1 ? wavenumber(kz, Nz, dz) : 0.0;
@@ -126,11 +135,12 @@ cudaError_t build_pml_deficit(float *out, int N, int pml_size, double alpha, dou
 }
 cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const double d[3],
                                  double c_ref, double dt, double c_sq_fold, int absorbing,
-                                 double tau, double eta, double y, cudaStream_t st) {
+                                 double tau, double eta, double y, const int *slot_ky,
+                                 cudaStream_t st) {
   const long long total = (long long)(N[0] / 2 + 1) * N[1] * N[2];
   k_build_eos_multiplier<<<blocks(total, 256), 256, 0, st>>>(M, M2, N[0], N[1], N[2], d[0],
                                                              d[1], d[2], c_ref, dt, c_sq_fold,
-                                                             absorbing, tau, eta, y);
+                                                             absorbing, tau, eta, y, slot_ky);
   return cudaGetLastError();
 }
 cudaError_t convert_f64_to_f32(float *out, const double *in, long long n, int op,
