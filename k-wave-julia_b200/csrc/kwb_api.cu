@@ -329,7 +329,7 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
     if (a >= h.ndim) continue;
     if ((e = launch_line_pass(S->d_sim, h, a, KWB_MODE_STEP, step_s, st)) != cudaSuccess) return e;
   }
-  if ((e = launch_eos_x_fwd(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
+  if (!h.fuse_xeos && (e = launch_eos_x_fwd(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
   if (h.ndim == 2) {
     if ((e = launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, step_s, st)) != cudaSuccess) return e;
   } else if (h.ndim == 3 && h.plane) {
@@ -348,7 +348,7 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
 }
 
 int count_launches(const kwb_sim *S) {
-  int n = (S->tr ? 1 : 0) + S->h.ndim + 2 + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? (S->h.plane ? 1 : 3) : 0));
+  int n = (S->tr ? 1 : 0) + S->h.ndim + (S->h.fuse_xeos ? 1 : 2) + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? (S->h.plane ? 1 : 3) : 0));
   for (auto &g : S->groups)
     if (!g.spec.cartesian && g.n > 0 && !g.fused) ++n;
   return n;
@@ -647,6 +647,10 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     const char *pv = getenv("KWB_PLANE");
     h.plane = (h.fast & 2) && D == 3 && !h.dispersion && fast_size(h.N[0]) && fast_plane_size(h.N[1], h.N[2]) &&
               !(pv && strcmp(pv, "0") == 0) && fast_plane_available();
+    // the x line pass carries the EOS x R2C when both run on the register-FFT kernels
+    // (KWB_FUSE_XEOS=0 keeps them separate)
+    const char *fx = getenv("KWB_FUSE_XEOS");
+    h.fuse_xeos = (h.fast & 3) == 3 && D >= 2 && !h.dispersion && fast_size(h.N[0]) && !(fx && strcmp(fx, "0") == 0);
   }
   {
     float *Mt, *M2 = nullptr;
@@ -1078,15 +1082,17 @@ int kwb_sim_profile(kwb_sim *S, int64_t steps, kwb_kernel_times *out) {
   for (long long i = 0; i < steps && err == cudaSuccess; ++i) {
     const long long s = S->steps_done - S->t0_host;
     if (S->tr) timed(slot("tr_inject", h.n_tr * 8.0), [&] { return launch_tr_inject(S->d_sim, h, s, st); });
+    const double eos_rd = nv * 4.0 * (h.D + (h.c0sq ? 1 : 0) + (h.nonlinear && h.nlq ? 1 : 0) + (h.dispersion ? 2 : 0));
     for (int a : {1, 2, 0}) {
       if (a >= h.ndim) continue;
       static const char *nm[3] = {"line_pass_x", "line_pass_y", "line_pass_z"};
-      timed(slot(nm[a], nv * 4.0 * (5 + hr)), [&] { return launch_line_pass(S->d_sim, h, a, KWB_MODE_STEP, s, st); });
+      // fused x pass: its own traffic plus the EOS forward's, less the rho_x it no longer re-reads
+      const double fused = (a == 0 && h.fuse_xeos) ? eos_rd - nv * 4.0 + ns * 8.0 : 0.0;
+      timed(slot(a == 0 && h.fuse_xeos ? "line_pass_x_eos_fwd" : nm[a], nv * 4.0 * (5 + hr) + fused),
+            [&] { return launch_line_pass(S->d_sim, h, a, KWB_MODE_STEP, s, st); });
     }
-    {
-      const double rd = nv * 4.0 * (h.D + (h.c0sq ? 1 : 0) + (h.nonlinear && h.nlq ? 1 : 0) + (h.dispersion ? 2 : 0));
-      timed(slot("eos_x_fwd", rd + ns * 8.0 * (h.dispersion ? 2 : 1)), [&] { return launch_eos_x_fwd(S->d_sim, h, s, st); });
-    }
+    if (!h.fuse_xeos)
+      timed(slot("eos_x_fwd", eos_rd + ns * 8.0 * (h.dispersion ? 2 : 1)), [&] { return launch_eos_x_fwd(S->d_sim, h, s, st); });
     if (h.ndim == 2) {
       timed(slot("spec_y_mul", ns * 8.0 * (h.dispersion ? 3 : 2) + ns * 4.0 * (h.dispersion ? 2 : 1)),
             [&] { return launch_spec_pass(S->d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, s, st); });

@@ -345,7 +345,10 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // fused per-axis line pass (same algorithm as kwb::k_line_pass)
 // ------------------------------------------------------------------------------------------
 
-template <class F, bool CONTIG, int LT, int MINB>
+// XEOS (x axis, time steps only): the pass ends with the equation of state's x R2C for its tile,
+// as k_eos_fwd_fast does, starting from rho_x still in registers (rho_y and rho_z are final:
+// the x pass runs last).
+template <class F, bool CONTIG, int LT, int MINB, bool XEOS>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_line_fast(const SimDev *__restrict__ sims, int axis, int mode, long long step_s) {
   constexpr int E = F::E, G = F::G;
@@ -577,6 +580,70 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   }
 #pragma unroll
   for (int r = 0; r < E; ++r) store_pair(rd, tt + G * r, v[r]);
+  if constexpr (XEOS) {
+    // equation of state, x R2C (k_eos_fwd_fast): sum of the split densities, nonlinearity, c^2
+#pragma unroll
+    for (int r = 0; r < E; ++r) v[r] = make_float2(va ? v[r].x : 0.f, vb ? v[r].y : 0.f);
+    if (S.D > 1) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const float2 b = load_pair(S.rho[1], tt + G * r);
+        v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+      }
+    }
+    if (S.D > 2) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const float2 b = load_pair(S.rho[2], tt + G * r);
+        v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+      }
+    }
+    if (S.nonlinear) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const float2 q = S.nlq ? load_pair(S.nlq, tt + G * r) : make_float2(S.nlq_s, S.nlq_s);
+        v[r] = make_float2(v[r].x * fmaf(q.x, v[r].x, 1.0f), v[r].y * fmaf(q.y, v[r].y, 1.0f));
+      }
+    }
+    if (S.c0sq) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const float2 c = load_pair(S.c0sq, tt + G * r);
+        v[r] = make_float2(c.x * v[r].x, c.y * v[r].y);
+      }
+    }
+    F::fwd(v, xs, tw2, tt);
+#pragma unroll
+    for (int idx = 0; idx < E; ++idx) xs[F::nat_of(tt, idx)] = v[idx];
+    {
+      const int n1 = S.n1, Ny = S.N[1];
+      const int rows = 2 * L, tpp = (Ny + rows - 1) / rows;
+      const int z = blockIdx.x / tpp, y0 = (blockIdx.x - z * tpp) * rows;
+      if (S.plane) {
+        __syncthreads();
+        for (int e = tid; e < n1 * L; e += blockDim.x) {
+          const int k = e / L, lp = e - k * L;
+          if (2 * lp >= cnt) continue;
+          const float2 *xl = sm + lp * LP;
+          const float2 zz = xl[F::nat(k)], zm = xl[F::nat(k == 0 ? 0 : N - k)];
+          float2 *dst = S.spec + ((long long)z * n1 + k) * Ny + y0 + 2 * lp;
+          const float2 A = make_float2(0.5f * (zz.x + zm.x), 0.5f * (zz.y - zm.y));
+          const float2 B = make_float2(0.5f * (zz.y + zm.y), -0.5f * (zz.x - zm.x));
+          if (2 * lp + 1 < cnt) *reinterpret_cast<float4 *>(dst) = make_float4(A.x, A.y, B.x, B.y);
+          else *dst = A;
+        }
+      } else {
+        F::sync();
+        const long long rowa = (long long)z * Ny + y0 + 2 * l;
+        for (int k = tt; k < n1; k += G) {
+          const float2 zz = xs[F::nat(k)];
+          const float2 zm = xs[F::nat(k == 0 ? 0 : N - k)];
+          if (va) S.spec[rowa * n1 + k] = make_float2(0.5f * (zz.x + zm.x), 0.5f * (zz.y - zm.y));
+          if (vb) S.spec[(rowa + 1) * n1 + k] = make_float2(0.5f * (zz.y + zm.y), -0.5f * (zz.x - zm.x));
+        }
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1060,7 +1127,9 @@ template <int N, bool C, int LT>
 static cudaError_t prime_line_variant() {
   using P = LinePolicy<N>;
   using F = typename P::template F<C>;
-  return raise_smem((const void *)k_line_fast<F, C, LT, P::MINB>, pline_smem<F>(LT));
+  cudaError_t e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, false>, pline_smem<F>(LT));
+  if (e != cudaSuccess || !C) return e;
+  return raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, true>, pline_smem<F>(LT));
 }
 
 template <int N>
@@ -1083,11 +1152,14 @@ static void line_go(const SimDev *d_sim, const SimDev &h, int axis, int mode, lo
   using P = LinePolicy<N>;
   if (axis == 0) {
     using F = typename P::template F<true>;
-    k_line_fast<F, true, LT, P::MINB><<<cdiv(h.N[1], 2 * LT) * h.N[2], LT * F::G, pline_smem<F>(LT), st>>>(
-        d_sim, axis, mode, s);
+    const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
+    if (h.fuse_xeos && mode == KWB_MODE_STEP)
+      k_line_fast<F, true, LT, P::MINB, true><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
+    else
+      k_line_fast<F, true, LT, P::MINB, false><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
   } else {
     using F = typename P::template F<false>;
-    k_line_fast<F, false, LT, P::MINB><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G,
+    k_line_fast<F, false, LT, P::MINB, false><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G,
                                          pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
   }
 }

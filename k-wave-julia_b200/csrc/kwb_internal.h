@@ -107,6 +107,8 @@ struct SimDev {
   // spectrum is then [z][kx][y] and M is [kx][k_z][slot] (slot: register order of the pass's y
   // transform, fast_plane_slot_ky)
   int plane;
+  // the x line pass ends with the equation of state's x R2C (no separate EOS forward pass)
+  int fuse_xeos;
 
   // A dense (every-voxel) sensor group recording only pressure fields, updated by the x C2R
   // pass as it writes p (no separate gather); nullptr when there is none.

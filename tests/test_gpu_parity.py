@@ -361,3 +361,16 @@ def test_plane_pass_matches_separate_passes(kb, wl, monkeypatch):
     assert l2 <= 1e-4, l2
     l2, _ = errors(plane.extra[0]["p_max"], sep.extra[0]["p_max"])
     assert l2 <= 1e-5, l2
+
+
+def test_fused_x_pass_and_eos_match_separate_kernels(kb, wl, monkeypatch):
+    """The x line pass carrying the EOS x R2C gives bit-identical fields to the separate kernels
+    (same operations in the same order), with and without the plane-major spectrum."""
+    for plane, case in (("1", wl.c3(n=256, Nt=30)), ("0", wl.c3(n=64, Nt=40, piston=8, pml=6))):
+        monkeypatch.setenv("KWB_PLANE", plane)
+        monkeypatch.delenv("KWB_FUSE_XEOS", raising=False)
+        fused = run_gpu(case)
+        monkeypatch.setenv("KWB_FUSE_XEOS", "0")
+        sep = run_gpu(case)
+        assert np.array_equal(fused["p"], sep["p"]), plane
+        assert np.array_equal(fused.extra[0]["p_max"], sep.extra[0]["p_max"]), plane
