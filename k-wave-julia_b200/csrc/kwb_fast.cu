@@ -38,6 +38,14 @@ __device__ constexpr float kSin64[32] = {
     7.0710678118654757e-01f, 6.3439328416364549e-01f, 5.5557023301960218e-01f, 4.7139673682599764e-01f,
     3.8268343236508978e-01f, 2.9028467725446233e-01f, 1.9509032201612825e-01f, 9.8017140329560604e-02f};
 
+// Packed FP32 pairs (FADD2 / FMUL2 / FFMA2): per component the same IEEE round-to-nearest
+// result as the scalar operation, in one instruction for both components.
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pair(float x) { return make_float2(x, x); }
+
 // x * exp(-+2 pi i j / 64), j a compile-time constant after unrolling
 template <bool INV>
 __device__ __forceinline__ float2 rot(float2 x, int j) {
@@ -68,8 +76,8 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[E]) {
 #pragma unroll
       for (int k = 0; k < span; ++k) {
         const float2 a = v[start + k], b = v[start + k + span];
-        v[start + k] = cadd(a, b);
-        v[start + k + span] = rot<INV>(csub(a, b), k * (32 / span));
+        v[start + k] = padd(a, b);
+        v[start + k + span] = rot<INV>(psub(a, b), k * (32 / span));
       }
     }
   }
@@ -204,7 +212,7 @@ struct LineFFT3 {
   __device__ __forceinline__ static void fwd(float2 (&v)[E], float2 *xs, const float2 *tw, int t) {
     dft_reg<R1, false>(v);
 #pragma unroll
-    for (int q = 0; q < R1; ++q) xs[i1(q, t)] = cmul(v[q], tw[q * RP + t]);
+    for (int q = 0; q < R1; ++q) xs[i1(q, t)] = q == 0 ? v[q] : cmul(v[q], tw[q * RP + t]);
     sync();
 #pragma unroll
     for (int j = 0; j < P2; ++j) {
@@ -214,7 +222,7 @@ struct LineFFT3 {
       for (int b = 0; b < B; ++b) w[b] = xs[i1(q1, a + A * b)];
       dft_reg<B, false>(w);
 #pragma unroll
-      for (int mb = 0; mb < B; ++mb) v[j * B + mb] = cmul(w[mb], tw[R1 * RP + mb * AP + a]);
+      for (int mb = 0; mb < B; ++mb) v[j * B + mb] = mb == 0 ? w[mb] : cmul(w[mb], tw[R1 * RP + mb * AP + a]);
     }
     sync();
 #pragma unroll
@@ -254,7 +262,7 @@ struct LineFFT3 {
       const int p = t * P2 + j, q1 = p / A, a = p - q1 * A;
       float2 w[B];
 #pragma unroll
-      for (int mb = 0; mb < B; ++mb) w[mb] = cmul_conj(xs[i2(q1, mb, a)], tw[R1 * RP + mb * AP + a]);
+      for (int mb = 0; mb < B; ++mb) w[mb] = mb == 0 ? xs[i2(q1, mb, a)] : cmul_conj(xs[i2(q1, mb, a)], tw[R1 * RP + mb * AP + a]);
       dft_reg<B, true>(w);
 #pragma unroll
       for (int b = 0; b < B; ++b) v[j * B + b] = w[b];
@@ -268,7 +276,7 @@ struct LineFFT3 {
     }
     sync();
 #pragma unroll
-    for (int q = 0; q < R1; ++q) v[q] = cmul_conj(xs[i1(q, t)], tw[q * RP + t]);
+    for (int q = 0; q < R1; ++q) v[q] = q == 0 ? xs[i1(q, t)] : cmul_conj(xs[i1(q, t)], tw[q * RP + t]);
     dft_reg<R1, true>(v);
     sync();
   }
@@ -486,12 +494,10 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     if (mode == KWB_MODE_INIT) {
       nv = make_float2(-0.5f * coef.x * v[r].x, -0.5f * coef.y * v[r].y);
     } else {
-      const float es = __ldg(esg + i);
+      const float2 nes = pair(-__ldg(esg + i));
       const float2 u0 = PF ? uu[PF ? r : 0] : load_pair(ud, i);
-      float ta = fmaf(-es, u0.x, u0.x), tb = fmaf(-es, u0.y, u0.y);
-      ta = fmaf(-coef.x, v[r].x, ta);
-      tb = fmaf(-coef.y, v[r].y, tb);
-      nv = make_float2(fmaf(-es, ta, ta), fmaf(-es, tb, tb));
+      const float2 tu = pfma(make_float2(-coef.x, -coef.y), v[r], pfma(nes, u0, u0));
+      nv = pfma(nes, tu, tu);
     }
     v[r] = make_float2(va ? nv.x : 0.f, vb ? nv.y : 0.f);
   }
@@ -546,19 +552,11 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
   for (int r = 0; r < E; ++r) {
     const int i = tt + G * r;
-    const float ei = __ldg(ed + i);
-    float2 coef;
-    if (rho0) {
-      const float2 r0 = staged(st_r, i);
-      coef = make_float2(S.dt * r0.x, S.dt * r0.y);
-    } else {
-      coef = make_float2(S.dt_rho0_s, S.dt_rho0_s);
-    }
+    const float2 nei = pair(-__ldg(ed + i));
+    const float2 ncoef = rho0 ? pmul(pair(-S.dt), staged(st_r, i)) : pair(-S.dt_rho0_s);
     const float2 r0d = staged(st_p, i);
-    float ta = fmaf(-ei, r0d.x, r0d.x), tb = fmaf(-ei, r0d.y, r0d.y);
-    ta = fmaf(-coef.x, v[r].x, ta);
-    tb = fmaf(-coef.y, v[r].y, tb);
-    v[r] = make_float2(fmaf(-ei, ta, ta), fmaf(-ei, tb, tb));
+    const float2 tr = pfma(ncoef, v[r], pfma(nei, r0d, r0d));
+    v[r] = pfma(nei, tr, tr);
   }
   // pressure (mass) sources (first_order_steps.jl:619-640, 692-715)
   if (S.n_p > 0 && S.p_line_ptr[axis]) {
@@ -588,28 +586,28 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const float2 b = load_pair(S.rho[1], tt + G * r);
-        v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+        v[r] = padd(v[r], b);
       }
     }
     if (S.D > 2) {
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const float2 b = load_pair(S.rho[2], tt + G * r);
-        v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+        v[r] = padd(v[r], b);
       }
     }
     if (S.nonlinear) {
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const float2 q = S.nlq ? load_pair(S.nlq, tt + G * r) : make_float2(S.nlq_s, S.nlq_s);
-        v[r] = make_float2(v[r].x * fmaf(q.x, v[r].x, 1.0f), v[r].y * fmaf(q.y, v[r].y, 1.0f));
+        v[r] = pmul(v[r], pfma(q, v[r], pair(1.0f)));
       }
     }
     if (S.c0sq) {
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const float2 c = load_pair(S.c0sq, tt + G * r);
-        v[r] = make_float2(c.x * v[r].x, c.y * v[r].y);
+        v[r] = pmul(c, v[r]);
       }
     }
     F::fwd(v, xs, tw2, tt);
@@ -684,28 +682,28 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const float2 b = ld(S.rho[1], tt + G * r);
-      v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+      v[r] = padd(v[r], b);
     }
   }
   if (S.D > 2) {
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const float2 b = ld(S.rho[2], tt + G * r);
-      v[r] = make_float2(v[r].x + b.x, v[r].y + b.y);
+      v[r] = padd(v[r], b);
     }
   }
   if (S.nonlinear) {
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const float2 q = S.nlq ? ld(S.nlq, tt + G * r) : make_float2(S.nlq_s, S.nlq_s);
-      v[r] = make_float2(v[r].x * fmaf(q.x, v[r].x, 1.0f), v[r].y * fmaf(q.y, v[r].y, 1.0f));
+      v[r] = pmul(v[r], pfma(q, v[r], pair(1.0f)));
     }
   }
   if (S.c0sq) {
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const float2 c = ld(S.c0sq, tt + G * r);
-      v[r] = make_float2(c.x * v[r].x, c.y * v[r].y);
+      v[r] = pmul(c, v[r]);
     }
   }
   __syncthreads();
@@ -1128,8 +1126,10 @@ static cudaError_t prime_line_variant() {
   using P = LinePolicy<N>;
   using F = typename P::template F<C>;
   cudaError_t e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, false>, pline_smem<F>(LT));
-  if (e != cudaSuccess || !C) return e;
-  return raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, true>, pline_smem<F>(LT));
+  if constexpr (C) {
+    if (e == cudaSuccess) e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, true>, pline_smem<F>(LT));
+  }
+  return e;
 }
 
 template <int N>
