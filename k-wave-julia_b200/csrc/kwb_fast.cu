@@ -358,7 +358,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // the x pass runs last).
 template <class F, bool CONTIG, int LT, int MINB, bool XEOS>
 __global__ void __launch_bounds__(LT * F::G, MINB)
-    k_line_fast(const SimDev *__restrict__ sims, int axis, int mode, long long step_s) {
+    k_line_fast(const __grid_constant__ SimDev S, int axis, int mode, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int RP = G + 1, LP = F::LP;
   constexpr int L = LT;  // complex lines per tile
@@ -367,13 +367,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   float2 *tw2 = sm + L * LP;
   float2 *gp2 = tw2 + F::TW;
   float2 *gn2 = gp2 + E * RP;
-  const SimDev &S = sims[0];
   const long long t = *S.t0 + step_s;
   if (mode == KWB_MODE_STEP && t >= S.Nt) return;
   const int tid = threadIdx.x;
   const int tt = CONTIG ? tid % G : tid / L;
   const int l = CONTIG ? tid / G : tid % L;
-  const int N = E * G;
+  constexpr int N = E * G, THREADS = LT * G;
   const int Nx = S.N[0];
 
   // tile geometry (as tile_x / tile_yz of the generic kernel, 2L real lines)
@@ -427,18 +426,30 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // strided [i][column] (the tile's own global layout, compacted).
   float *st_p = reinterpret_cast<float *>(reinterpret_cast<char *>(smem_raw) + pline_offset<F>(L));
   float *st_r = st_p + 2 * L * N;
+  // Chunk assignments are compile-time strides from a per-thread start, so the addresses of a
+  // thread's chunks differ by constants.
   auto stage = [&](float *dst, const float *f) {
     const float *fb = f + base;
     if (CONTIG) {
-      const int chunks = cnt * N / 4;  // the tile's rows are contiguous in memory
-      for (int q = tid; q < chunks; q += blockDim.x) cp_async16(dst + 4 * q, fb + 4 * q, 16);
+      constexpr int CH = 2 * L * N / 4, PER = (CH + THREADS - 1) / THREADS;  // rows contiguous in memory
+      const int chunks = cnt * N / 4;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int q = tid + k * THREADS;
+        if (q < chunks) cp_async16(dst + 4 * q, fb + 4 * q, 16);
+      }
     } else {
       constexpr int CPR = (2 * L) / 4;  // 16-byte chunks per tile row (strided tiles have L >= 2)
-      for (int q = tid; q < CPR * N; q += blockDim.x) {
-        const int i = q / CPR, ch = q - i * CPR;
-        const int valid = min(4, cnt - 4 * ch);
-        cp_async16(dst + i * 2 * L + 4 * ch, fb + (long long)i * st32 + 4 * ch, valid > 0 ? 4 * valid : 0);
-      }
+      static_assert(THREADS % CPR == 0 && (CPR * N) % THREADS == 0, "strided staging");
+      constexpr int RSTEP = THREADS / CPR, PER = CPR * N / THREADS;
+      const int ch = tid % CPR, i0 = tid / CPR;
+      const int valid = min(4, cnt - 4 * ch);
+      const int bytes = valid > 0 ? 4 * valid : 0;
+      float *d0 = dst + i0 * 2 * L + 4 * ch;
+      const float *s0 = fb + i0 * st32 + 4 * ch;
+      const int sstep = RSTEP * st32;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) cp_async16(d0 + k * RSTEP * 2 * L, s0 + k * sstep, bytes);
     }
     cp_async_commit();
   };
@@ -482,7 +493,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
   for (int r = 0; r < E; ++r) {
     const int i = tt + G * r;
-    const int inext = (i + 1 == N) ? 0 : i + 1;
+    const int inext = (r == E - 1 && tt == G - 1) ? 0 : i + 1;  // periodic neighbour
     float2 coef;
     if (rho0) {
       const float2 r0 = staged(st_r, i), r1 = staged(st_r, inext);
@@ -652,13 +663,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 // [z][y][kx].
 template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
-    k_eos_fwd_fast(const SimDev *__restrict__ sims, long long step_s) {
+    k_eos_fwd_fast(const __grid_constant__ SimDev S, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
-  const SimDev &S = sims[0];
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;
   const int tid = threadIdx.x, tt = tid % G, l = tid / G;
@@ -741,13 +751,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 
 template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
-    k_eos_inv_fast(const SimDev *__restrict__ sims, long long step_s) {
+    k_eos_inv_fast(const __grid_constant__ SimDev S, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
-  const SimDev &S = sims[0];
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;
   const int tid = threadIdx.x, tt = tid % G, l = tid / G;
@@ -853,13 +862,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 
 template <class F, int LT, int MINB>
 __global__ void __launch_bounds__(LT * F::G, MINB)
-    k_spec_fast(const SimDev *__restrict__ sims, int axis, int op, long long step_s) {
+    k_spec_fast(const __grid_constant__ SimDev S, int axis, int op, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
-  const SimDev &S = sims[0];
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;
   const int tid = threadIdx.x, l = tid % L, tt = tid / L;
@@ -960,7 +968,7 @@ __device__ __forceinline__ unsigned cluster_rank() {
 // The spectrum crosses HBM once in and once out per step, with the multiplier read once.
 template <class FY, class FZ, int CL>
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 2)
-    k_plane_fast(const SimDev *__restrict__ sims, long long step_s) {
+    k_plane_fast(const __grid_constant__ SimDev S, long long step_s) {
   constexpr int NY = FY::N, NZ = FZ::N, RZ = NZ / CL, CY = NY / CL;
   constexpr int LY = KWB_PLANE_THREADS / FY::G, LZ = KWB_PLANE_THREADS / FZ::G;
   static_assert(RZ == 2 * LY && CY % LZ == 0 && RZ == FZ::G, "plane tiling");
@@ -970,7 +978,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 
   float2 *xsb = data + RZ * NY;
   float2 *twy = xsb + XS;
   float2 *twz = twy + FY::TW;
-  const SimDev &S = sims[0];
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;  // uniform over the cluster
   const unsigned rank = cluster_rank();
@@ -1154,13 +1161,13 @@ static void line_go(const SimDev *d_sim, const SimDev &h, int axis, int mode, lo
     using F = typename P::template F<true>;
     const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
     if (h.fuse_xeos && mode == KWB_MODE_STEP)
-      k_line_fast<F, true, LT, P::MINB, true><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
+      k_line_fast<F, true, LT, P::MINB, true><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(h, axis, mode, s);
     else
-      k_line_fast<F, true, LT, P::MINB, false><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
+      k_line_fast<F, true, LT, P::MINB, false><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(h, axis, mode, s);
   } else {
     using F = typename P::template F<false>;
     k_line_fast<F, false, LT, P::MINB, false><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G,
-                                         pline_smem<F>(LT), st>>>(d_sim, axis, mode, s);
+                                         pline_smem<F>(LT), st>>>(h, axis, mode, s);
   }
 }
 
@@ -1216,11 +1223,11 @@ static void eos_go(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, 
   using F = typename P::template F<true>;
   const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
   if (h.plane) {
-    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
-    else k_eos_inv_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
+    else k_eos_inv_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
   } else {
-    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
-    else k_eos_inv_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, s);
+    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
+    else k_eos_inv_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
   }
 }
 
@@ -1243,7 +1250,7 @@ static void spec_go(const SimDev *d_sim, const SimDev &h, int axis, int op, long
   using P = LinePolicy<N>;
   using F = typename P::template F<false>;
   const int grid = cdiv(h.n1, LT) * (axis == 1 ? h.N[2] : h.N[1]);
-  k_spec_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(d_sim, axis, op, s);
+  k_spec_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, axis, op, s);
 }
 
 template <int N>
@@ -1306,7 +1313,7 @@ void fast_plane_slot_ky(int Ny, int *ky) {
 }
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
   fast::k_plane_fast<fast::PlaneFY, fast::PlaneFZ, fast::kPlaneCL>
-      <<<h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st>>>(d_sim, s);
+      <<<h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st>>>(h, s);
   return cudaGetLastError();
 }
 
