@@ -529,13 +529,15 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   }
 
   // velocity sources on this tile's lines (first_order_steps.jl:586-617, 646-690)
-  if (S.u_sig[axis] && S.u_line_ptr[axis]) {
+  // (entries are sorted by line: a thread scans only its own two lines)
+  if (S.u_sig[axis] && S.u_line_ptr[axis] && va) {
     const int tcol = (int)(min(t + 1, (long long)S.u_cols[axis]) - 1);
-    const int q0 = S.u_line_ptr[axis][first_line], q1 = S.u_line_ptr[axis][first_line + cnt];
+    const int la = first_line + 2 * l;
+    const int q0 = S.u_line_ptr[axis][la], q1 = S.u_line_ptr[axis][la + (vb ? 2 : 1)];
     for (int q = q0; q < q1; ++q) {
       const SrcEntry se = S.u_entry[axis][q];
-      const int c = se.line - first_line;
-      if ((c >> 1) != l || (se.pos % G) != tt) continue;
+      const int c = se.line - la;
+      if ((se.pos % G) != tt) continue;
       const int ro = se.pos / G;
       const float val = S.u_sig[axis][(long long)tcol * S.n_u + se.j];
 #pragma unroll
@@ -570,13 +572,14 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     v[r] = pfma(nei, tr, tr);
   }
   // pressure (mass) sources (first_order_steps.jl:619-640, 692-715)
-  if (S.n_p > 0 && S.p_line_ptr[axis]) {
+  if (S.n_p > 0 && S.p_line_ptr[axis] && va) {
     const int tcol = (int)(min(t + 1, (long long)S.p_cols) - 1);
-    const int q0 = S.p_line_ptr[axis][first_line], q1 = S.p_line_ptr[axis][first_line + cnt];
+    const int la = first_line + 2 * l;
+    const int q0 = S.p_line_ptr[axis][la], q1 = S.p_line_ptr[axis][la + (vb ? 2 : 1)];
     for (int q = q0; q < q1; ++q) {
       const SrcEntry se = S.p_entry[axis][q];
-      const int c = se.line - first_line;
-      if ((c >> 1) != l || (se.pos % G) != tt) continue;
+      const int c = se.line - la;
+      if ((se.pos % G) != tt) continue;
       const int ro = se.pos / G;
       const float val = S.p_sig[(long long)tcol * S.n_p + se.j];
 #pragma unroll
@@ -630,12 +633,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
       const int z = blockIdx.x / tpp, y0 = (blockIdx.x - z * tpp) * rows;
       if (S.plane) {
         __syncthreads();
-        for (int e = tid; e < n1 * L; e += blockDim.x) {
-          const int k = e / L, lp = e - k * L;
-          if (2 * lp >= cnt) continue;
-          const float2 *xl = sm + lp * LP;
+        const int lp = tid % L;
+        const float2 *xl = sm + lp * LP;
+        float2 *dst = S.spec + ((long long)z * n1 + tid / L) * Ny + y0 + 2 * lp;
+        const long long kstep = (long long)G * Ny;  // THREADS / L = G values of kx per sweep
+        for (int k = tid / L; k < n1 && 2 * lp < cnt; k += G, dst += kstep) {
           const float2 zz = xl[F::nat(k)], zm = xl[F::nat(k == 0 ? 0 : N - k)];
-          float2 *dst = S.spec + ((long long)z * n1 + k) * Ny + y0 + 2 * lp;
           const float2 A = make_float2(0.5f * (zz.x + zm.x), 0.5f * (zz.y - zm.y));
           const float2 B = make_float2(0.5f * (zz.y + zm.y), -0.5f * (zz.x - zm.x));
           if (2 * lp + 1 < cnt) *reinterpret_cast<float4 *>(dst) = make_float4(A.x, A.y, B.x, B.y);
@@ -726,12 +729,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     // one (kx, line pair) per thread, pairs fastest: the pair's two rows are adjacent in y, so
     // each thread writes A and B as one 16-byte store and each kx gets 2L consecutive y
     __syncthreads();
-    for (int e = tid; e < n1 * L; e += blockDim.x) {
-      const int k = e / L, lp = e - k * L;
-      if (2 * lp >= cnt) continue;
-      const float2 *xl = sm + lp * LP;
+    const int lp = tid % L;
+    const float2 *xl = sm + lp * LP;
+    float2 *dst = S.spec + ((long long)z * n1 + tid / L) * Ny + y0 + 2 * lp;
+    const long long kstep = (long long)G * Ny;  // THREADS / L = G values of kx per sweep
+    for (int k = tid / L; k < n1 && 2 * lp < cnt; k += G, dst += kstep) {
       const float2 zz = xl[F::nat(k)], zm = xl[F::nat(k == 0 ? 0 : N - k)];
-      float2 *dst = S.spec + ((long long)z * n1 + k) * Ny + y0 + 2 * lp;
       const float2 A = make_float2(0.5f * (zz.x + zm.x), 0.5f * (zz.y - zm.y));
       const float2 B = make_float2(0.5f * (zz.y + zm.y), -0.5f * (zz.x - zm.x));
       if (2 * lp + 1 < cnt) *reinterpret_cast<float4 *>(dst) = make_float4(A.x, A.y, B.x, B.y);
@@ -772,9 +775,11 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   if (PLANE) {
     // one (kx, line pair) per thread, pairs fastest: the pair's rows are adjacent in y, so A and
     // B arrive as one 16-byte load and each kx reads 2L consecutive y
-    for (int e = tid; e < n1 * L; e += blockDim.x) {
-      const int k = e / L, lp = e - k * L;
-      const float2 *srcp = S.spec + ((long long)z * n1 + k) * Ny + y0 + 2 * lp;
+    const int lp = tid % L;
+    float2 *xl = sm + lp * LP;
+    const float2 *srcp = S.spec + ((long long)z * n1 + tid / L) * Ny + y0 + 2 * lp;
+    const long long kstep = (long long)G * Ny;  // THREADS / L = G values of kx per sweep
+    for (int k = tid / L; k < n1; k += G, srcp += kstep) {
       float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
       if (2 * lp + 1 < cnt) {
         const float4 ab = *reinterpret_cast<const float4 *>(srcp);
@@ -783,7 +788,6 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
       } else if (2 * lp < cnt) {
         A = *srcp;
       }
-      float2 *xl = sm + lp * LP;
       if (k == 0 || 2 * k == N) {
         xl[F::nat(k)] = make_float2(A.x, B.x);  // c2r ignores Im of the DC and Nyquist bins
       } else {
@@ -831,32 +835,46 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   }
   F::sync();
   F::inv(v, xs, tw2, tt);
-  float *__restrict__ p = S.p;
-#pragma unroll
-  for (int r = 0; r < E; ++r) {
-    const int i = tt + G * r;
-    if (va) p[ra + i] = v[r].x;
-    if (vb) p[rb + i] = v[r].y;
-  }
-  if (gm) {
-    const bool last = (t == S.Nt - 1);
+  // p and the dense sensor fields: one pass per field over this thread's two rows (ra, ra + N)
+  auto put = [&](float *a) {
 #pragma unroll
     for (int r = 0; r < E; ++r) {
-      const int i = tt + G * r;
+      if (va) a[tt + G * r] = v[r].x;
+      if (vb) a[N + tt + G * r] = v[r].y;
+    }
+  };
+  put(S.p + ra);
+  if (gm) {
+    if (gm & (1u << 0)) put(gd->ser_p + t * gd->n + ra);
+    if (gm & (1u << 1)) {
+      float *a = gd->pmax + ra;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (!(h ? vb : va)) continue;
-        const long long vx = (h ? rb : ra) + i;
-        const float pv = h ? v[r].y : v[r].x;
-        if (gm & (1u << 0)) gd->ser_p[t * gd->n + vx] = pv;
-        if (gm & (1u << 1))
-          gd->pmax[vx] = fmaxf(PFS ? (h ? pm[PFS ? r : 0].y : pm[PFS ? r : 0].x) : gd->pmax[vx], pv);
-        if (gm & (1u << 2))
-          gd->pmin[vx] = fminf(PFS ? (h ? pn[PFS ? r : 0].y : pn[PFS ? r : 0].x) : gd->pmin[vx], pv);
-        if (gm & (1u << 3)) gd->prms[vx] += (double)gd->cnt_prms * ((double)pv * (double)pv);
-        if ((gm & (1u << 4)) && last) gd->pfinal[vx] = pv;
+      for (int r = 0; r < E; ++r) {
+        const int i = tt + G * r;
+        if (va) a[i] = fmaxf(PFS ? pm[PFS ? r : 0].x : a[i], v[r].x);
+        if (vb) a[N + i] = fmaxf(PFS ? pm[PFS ? r : 0].y : a[N + i], v[r].y);
       }
     }
+    if (gm & (1u << 2)) {
+      float *a = gd->pmin + ra;
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const int i = tt + G * r;
+        if (va) a[i] = fminf(PFS ? pn[PFS ? r : 0].x : a[i], v[r].x);
+        if (vb) a[N + i] = fminf(PFS ? pn[PFS ? r : 0].y : a[N + i], v[r].y);
+      }
+    }
+    if (gm & (1u << 3)) {
+      double *a = gd->prms + ra;
+      const double w = (double)gd->cnt_prms;
+#pragma unroll
+      for (int r = 0; r < E; ++r) {
+        const int i = tt + G * r;
+        if (va) a[i] += w * ((double)v[r].x * (double)v[r].x);
+        if (vb) a[N + i] += w * ((double)v[r].y * (double)v[r].y);
+      }
+    }
+    if ((gm & (1u << 4)) && t == S.Nt - 1) put(gd->pfinal + ra);
   }
 }
 

@@ -181,6 +181,24 @@ def test_velocity_sources_2d_additive_and_dirichlet(kb):
         assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
 
 
+def test_pressure_sources_2d_register_sizes(kb):
+    """Mass sources on a 64^2 grid (register-FFT kernels): a 4 x 4 block, several points per line
+    on both axes, additive and Dirichlet."""
+    from kwave_b200.workloads import Case
+    n = 64
+    dt = 0.3e-4 / 1500
+    t = np.arange(160) * dt
+    pm = np.zeros((n, n), bool)
+    pm[28:32, 30:34] = True
+    sig = np.vstack([np.sin(2 * math.pi * (1 + 0.1 * j) * 1e6 * t) for j in range(16)])
+    mask = np.zeros((n, n), bool)
+    mask[44, 31] = mask[31, 50] = mask[10, 10] = True
+    for mode in (kb.Additive, kb.Dirichlet):
+        case = Case("psrc", (n, n), (1e-4, 1e-4), dt, 160, dict(sound_speed=1500.0, density=1000.0),
+                    dict(p_mask=pm, p=sig, p_mode=mode), dict(mask=mask, record=["p", "p_final"]))
+        assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
+
+
 def test_velocity_recording_3d(kb):
     """test_solver_3d.jl:74-98 restated: 24^3 ball p0, record p, ux, uy, uz, u_max."""
     from kwave_b200.workloads import Case
