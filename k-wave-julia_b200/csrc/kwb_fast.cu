@@ -464,19 +464,17 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
   float2 *xs = sm + l * LP;
   float *__restrict__ ud = S.u[axis];
-  // velocity prefetch ahead of the transform arithmetic (contiguous tiles; strided tiles load
-  // it where it is used, to stay within 64 registers)
-  constexpr bool PF = CONTIG && E <= 16;
-  float2 uu[PF ? E : 1];
-  if (PF && mode == KWB_MODE_STEP) {
-#pragma unroll
-    for (int r = 0; r < E; ++r) uu[PF ? r : 0] = load_pair(ud, tt + G * r);
-  }
   cp_async_wait<1>();  // the p tile has landed (rho0 may still be in flight)
   __syncthreads();     // ... for every thread; tables too
   float2 v[E];
 #pragma unroll
   for (int r = 0; r < E; ++r) v[r] = staged(st_p, tt + G * r);
+  // time steps: the velocity tile takes the p tile's slot while d/dx_d p is transformed
+  // (INIT keeps p staged: it is read again below)
+  if (mode == KWB_MODE_STEP) {
+    __syncthreads();  // every thread has its p values
+    stage(st_p, ud);
+  }
 
   // d/dx_d p  (staggered +)
   F::fwd(v, xs, tw2, tt);
@@ -484,9 +482,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gp2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
   cp_async_wait<0>();
-  __syncthreads();  // the rho0 tile has landed; every thread is done with the p tile
-  // the split density rho_d goes into the p tile's slot while d/dx_d u is transformed
-  if (mode == KWB_MODE_STEP) stage(st_p, S.rho[axis]);
+  __syncthreads();  // the rho0 and velocity tiles have landed
 
   // velocity update u = pml_sg (pml_sg u - dt/rho_sg dp)
   const float *__restrict__ esg = S.pml_sg_def[axis];
@@ -506,7 +502,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
       nv = make_float2(-0.5f * coef.x * v[r].x, -0.5f * coef.y * v[r].y);
     } else {
       const float2 nes = pair(-__ldg(esg + i));
-      const float2 u0 = PF ? uu[PF ? r : 0] : load_pair(ud, i);
+      const float2 u0 = staged(st_p, i);
       const float2 tu = pfma(make_float2(-coef.x, -coef.y), v[r], pfma(nes, u0, u0));
       nv = pfma(nes, tu, tu);
     }
@@ -527,6 +523,10 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     (void)invD;
     return;
   }
+
+  // the split density rho_d takes the slot while d/dx_d u is transformed
+  __syncthreads();  // every thread is done with the velocity tile
+  stage(st_p, S.rho[axis]);
 
   // velocity sources on this tile's lines (first_order_steps.jl:586-617, 646-690)
   // (entries are sorted by line: a thread scans only its own two lines)
