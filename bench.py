@@ -25,6 +25,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "k-wave-julia_b200"))
 
 # Spectral-pass-model words per voxel-step (algorithmic bytes = 4 B x words), per config.
+
+# DRAM bytes read + written (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# dominant kernel, from one `ncu --set full --clock-control none` capture of time step 2 of
+# `bench.py --steps 4 --warmup 3 --no-e2e --no-cpu --no-batch --no-serve` on a B200.  Reads
+# equal the algorithmic bytes; writes land lower because part of each launch's output is still
+# in L2 when the launch ends.
+NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 710.85e6}
+
 SPM_WORDS = {"c3": 33.0, "c2": 26.0, "c1": 15.01}
 UNIT = "Gvoxel-steps/s"
 METRIC = "Gvoxel-steps/s (fluid k-space time stepping)"
@@ -199,7 +207,7 @@ def batch_bench(ctx, n_sims=64):
             "results_identical_to_alone": bool(same)}
 
 
-def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800)):
+def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800), max_running=64, one_at_a_time=True):
     """Config 5: Poisson arrivals (mean rate 200/s) of mixed 2D/3D requests; latency is arrival to
     completion.  The comparison serves the same arrivals one at a time with blocking solves."""
     import threading
@@ -218,7 +226,7 @@ def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800)):
         return out
 
     preps = prep_all()
-    kb.serving_config(max_running=64, chunk_steps=32, context=ctx)
+    kb.serving_config(max_running=max_running, chunk_steps=32, context=ctx)
     reqs = [None] * n_req
     t0 = time.perf_counter()
 
@@ -239,6 +247,13 @@ def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800)):
         lat.append((r.info["end_ns"] - r.info["submit_ns"]) / 1e9)
     t_end = max(t0 + arrivals[i] + lat[i] for i in range(n_req))
     span = t_end - t0
+    q = lambda a, x: float(np.percentile(np.asarray(a), x))
+    res = {"workload": f"{n_req} Poisson requests at {rate:.0f}/s, 70% 2D 256-1024 / 30% 3D 64^3-192^3, "
+                       f"Nt {nt_range[0]}-{nt_range[1]}",
+           "max_running": max_running,
+           "sims_per_s": n_req / span, "p50_latency_s": q(lat, 50), "p99_latency_s": q(lat, 99)}
+    if not one_at_a_time:
+        return res
     preps1 = prep_all()
     t0 = time.perf_counter()
     lat1 = []
@@ -249,12 +264,8 @@ def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800)):
         kb.solve_prepared(p)
         lat1.append(time.perf_counter() - (t0 + arrivals[i]))
     span1 = time.perf_counter() - t0
-    q = lambda a, x: float(np.percentile(np.asarray(a), x))
-    return {"workload": f"{n_req} Poisson requests at {rate:.0f}/s, 70% 2D 256-1024 / 30% 3D 64^3-192^3, "
-                        f"Nt {nt_range[0]}-{nt_range[1]}",
-            "sims_per_s": n_req / span, "p50_latency_s": q(lat, 50), "p99_latency_s": q(lat, 99),
-            "one_at_a_time": {"sims_per_s": n_req / span1, "p50_latency_s": q(lat1, 50),
-                              "p99_latency_s": q(lat1, 99)}}
+    res["one_at_a_time"] = {"sims_per_s": n_req / span1, "p50_latency_s": q(lat1, 50), "p99_latency_s": q(lat1, 99)}
+    return res
 
 
 def main():
@@ -346,7 +357,10 @@ def main():
                        "l2": "inputs larger than L2 (7 FP32 state fields + medium, > 126 MB)",
                        "timing": "CUDA events on the simulation stream, CUDA-graph replay of 32-step chunks"},
             "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC.get((args.config, dom["name"])),
+                         "traffic_unit": "DRAM bytes read + written per launch (ncu)",
+                         "algorithmic_bytes": dom["bytes_per_launch"],
                          "peak_kind": f"{peak_kind} copy bandwidth (burst)"},
             "spm": {"bytes_per_voxel_step": spm_bytes, "achieved_GBps": spm_bytes * value * 1e9 / world / 1e9,
                     "frac": spm_frac},
