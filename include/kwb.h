@@ -119,6 +119,12 @@ typedef struct kwb_problem {
   const kwb_sensor_group *groups;
 
   kwb_progress_fn progress; void *progress_user;
+
+  /* Memory order of the grid-shaped arrays (c0, rho0, BonA, p0): 0 = column-major, the
+   * reference's Julia order (x fastest); 1 = row-major, NumPy's default (the last axis
+   * fastest).  Row-major arrays are uploaded as they are and reordered on the device.  Index
+   * lists (p_index, u_index, sensor indices) are column-major linear indices either way. */
+  int32_t row_major;
 } kwb_problem;
 
 /* Output sizes of one group: rows x cols per field, 0 x 0 when the field is not recorded. */
@@ -214,8 +220,9 @@ typedef struct kwb_serving_stats {
   int64_t queued, running, running_bytes;
 } kwb_serving_stats;
 
-/* Scheduler limits: at most `max_running` admitted simulations, `chunk_steps` time steps per
- * launch, and (if > 0) at most `mem_cap_bytes` of modelled device memory in use. */
+/* Scheduler limits: at most `max_running` admitted simulations (default 8), `chunk_steps` time
+ * steps per launch (default 32), and (if > 0) at most `mem_cap_bytes` of modelled device memory
+ * in use. */
 int kwb_serving_config(kwb_ctx *ctx, int32_t max_running, int32_t chunk_steps, int64_t mem_cap_bytes);
 int kwb_submit(kwb_ctx *ctx, const kwb_problem *problem, kwb_outputs *outputs, uint64_t *ticket);
 /* *done = 1 once the request has completed (successfully or not). */

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/kwb.h"
@@ -23,6 +24,18 @@ struct kwb_ctx {
   int device = 0;
   std::string err;
   KwbServer *server = nullptr;  // started by the first kwb_submit
+  // pinned staging for device -> host read-back (two halves), allocated on first use
+  float *pin = nullptr;
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+  // Device memory pool of this context's simulations: stream-ordered allocation, and freed
+  // blocks stay in the pool for the next simulation (no unmapping between simulations).
+  cudaMemPool_t pool = nullptr;
+  ~kwb_ctx() {
+    if (pool) cudaMemPoolDestroy(pool);  // released once outstanding blocks are freed
+    if (pin) cudaFreeHost(pin);
+    for (cudaEvent_t e : pin_ev)
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 size_t estimate_device_bytes(const kwb_problem *P);
@@ -45,6 +58,25 @@ int set_err(kwb_ctx *ctx, int code, const char *fmt, ...) {
   return code;
 }
 
+// Split [0, n) over host threads (one thread below 256K elements per thread).
+template <class Fn>
+void parallel_range(long long n, Fn fn) {
+  const long long hw = std::max(1u, std::min(std::thread::hardware_concurrency(), 16u));
+  const long long T = std::min(hw, (n + (1 << 18) - 1) >> 18);
+  if (T <= 1) {
+    fn(0LL, n);
+    return;
+  }
+  const long long per = (n + T - 1) / T;
+  std::vector<std::thread> th;
+  for (long long k = 1; k < T; ++k) {
+    const long long lo = k * per, hi = std::min(n, lo + per);
+    if (lo < hi) th.emplace_back(fn, lo, hi);
+  }
+  fn(0LL, std::min(n, per));
+  for (auto &x : th) x.join();
+}
+
 #define CU(call)                                                                        \
   do {                                                                                  \
     cudaError_t e_ = (call);                                                            \
@@ -52,6 +84,36 @@ int set_err(kwb_ctx *ctx, int code, const char *fmt, ...) {
       return set_err(ctx, KWB_E_DEVICE, "CUDA error %s at %s:%d (%s)",                  \
                      cudaGetErrorString(e_), __FILE__, __LINE__, #call);                \
   } while (0)
+
+// Device FP32 array -> caller's FP64 array in chunks through the context's pinned buffer: the
+// next chunk's copy (on `st`) overlaps this chunk's conversion, which runs on host threads (and
+// so also takes the first-touch page faults of a freshly allocated destination in parallel).
+constexpr long long kPinFloats = 8LL << 20;  // floats per half of the pinned buffer (32 MB)
+int read_f32_as_f64(kwb_ctx *ctx, cudaStream_t st, const float *src, long long cnt, double *dst) {
+  if (cnt <= 0) return KWB_OK;
+  if (!ctx->pin) {
+    CU(cudaMallocHost(&ctx->pin, 2 * kPinFloats * sizeof(float)));
+    for (cudaEvent_t &e : ctx->pin_ev) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const long long nch = (cnt + kPinFloats - 1) / kPinFloats;
+  auto issue = [&](long long c) -> cudaError_t {
+    const long long lo = c * kPinFloats, len = std::min(kPinFloats, cnt - lo);
+    cudaError_t e = cudaMemcpyAsync(ctx->pin + (c & 1) * kPinFloats, src + lo, len * 4, cudaMemcpyDeviceToHost, st);
+    return e == cudaSuccess ? cudaEventRecord(ctx->pin_ev[c & 1], st) : e;
+  };
+  CU(issue(0));
+  for (long long c = 0; c < nch; ++c) {
+    CU(cudaEventSynchronize(ctx->pin_ev[c & 1]));
+    if (c + 1 < nch) CU(issue(c + 1));
+    const long long lo = c * kPinFloats, len = std::min(kPinFloats, cnt - lo);
+    const float *sp = ctx->pin + (c & 1) * kPinFloats;
+    double *dp = dst + lo;
+    parallel_range(len, [sp, dp](long long a, long long b) {
+      for (long long i = a; i < b; ++i) dp[i] = (double)sp[i];
+    });
+  }
+  return KWB_OK;
+}
 
 // Julia's mean() sums pairwise; a pairwise sum keeps c_ref at FP64 round-off as well.
 double pairwise_sum(const double *x, long long n) {
@@ -98,17 +160,48 @@ int choose_L(int N, int want, int cap_lines, int dispersion, bool spec) {
   return L;
 }
 
-struct DevBuf {
+// Stream-ordered device scratch for simulation set-up (FP64 staging of the medium): freed on
+// the set-up stream when the creating call returns, so it holds no memory afterwards.
+struct TempBuf {
+  cudaStream_t st = nullptr;
+  cudaMemPool_t pool = nullptr;
   std::vector<void *> ptrs;
-  size_t bytes = 0;
-  ~DevBuf() {
-    for (void *p : ptrs) cudaFree(p);
+  TempBuf(cudaStream_t s, cudaMemPool_t p) : st(s), pool(p) {}
+  ~TempBuf() {
+    for (void *p : ptrs) cudaFreeAsync(p, st);
   }
   template <class T>
   cudaError_t alloc(T **out, size_t count) {
     void *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, (count ? count : 1) * sizeof(T), pool, st);
+    if (e != cudaSuccess) return e;
+    ptrs.push_back(p);
+    *out = static_cast<T *>(p);
+    return cudaSuccess;
+  }
+};
+
+// A simulation's device buffers, allocated and released in stream order on its stream (`st`):
+// releasing them does not wait for the rest of the device, unlike cudaFree, so retiring one of
+// many concurrent simulations does not stall the others.
+struct DevBuf {
+  std::vector<void *> ptrs;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  cudaMemPool_t pool = nullptr;
+  void release() {
+    for (void *p : ptrs) {
+      if (st) cudaFreeAsync(p, st);
+      else cudaFree(p);
+    }
+    ptrs.clear();
+  }
+  ~DevBuf() { release(); }
+  template <class T>
+  cudaError_t alloc(T **out, size_t count) {
+    void *p = nullptr;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    cudaError_t e = st ? cudaMallocFromPoolAsync(&p, count * sizeof(T), pool, st) : cudaMalloc(&p, count * sizeof(T));
     if (e != cudaSuccess) return e;
     ptrs.push_back(p);
     bytes += count * sizeof(T);
@@ -161,6 +254,7 @@ struct kwb_sim {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (p_host) cudaFreeHost(p_host);
+    mem.release();  // stream-ordered, before the stream goes
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -373,7 +467,9 @@ size_t estimate_device_bytes(const kwb_problem *P) {
   if (dispersion) need += (size_t)nvox * 4 + (size_t)nspec * 8;
   need += (size_t)nspec * 4 * (dispersion ? 2 : 1);
   need += (size_t)nvox * 4 * ((r_arr ? 1 : 0) + (c_arr ? 1 : 0) + ((nonlinear && (b_arr || r_arr)) ? 1 : 0));
-  if (c_arr || r_arr || b_arr || P->p0.count) need += (size_t)nvox * 8 * ((nonlinear && b_arr && r_arr) ? 2 : 1);
+  // FP64 staging during set-up (released once the simulation is created)
+  if (c_arr || r_arr || b_arr || P->p0.count)
+    need += (size_t)nvox * 8 * (((nonlinear && b_arr && r_arr) ? 2 : 1) + ((P->row_major && D > 1) ? 1 : 0));
   for (int g = 0; g < P->n_groups; ++g) {
     const kwb_sensor_group &G = P->groups[g];
     if (G.cartesian) continue;
@@ -478,7 +574,18 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   CU(cudaSetDevice(ctx->device));
   std::unique_ptr<kwb_sim> S(new kwb_sim());
   S->ctx = ctx;
+  if (!ctx->pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    CU(cudaMemPoolCreate(&ctx->pool, &props));
+    uint64_t keep = UINT64_MAX;  // hold freed blocks for reuse until the context goes
+    CU(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  S->mem.st = S->stream;
+  S->mem.pool = ctx->pool;
   CU(cudaEventCreate(&S->ev0));
   CU(cudaEventCreate(&S->ev1));
   cudaStream_t st = S->stream;
@@ -505,6 +612,8 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   const bool b_arr = P->BonA.count == nvox && nvox > 1;
   const double c_s = P->c0.data[0];
   const double r_s = P->rho0.count ? P->rho0.data[0] : 1.0;
+  // (in memory order: for row-major input the summation order differs from the reference's
+  // column-major one, which changes c_ref only at FP64 round-off)
   const double c_ref = c_arr ? pairwise_sum(P->c0.data, nvox) / (double)nvox : c_s;
   const bool absorbing = P->alpha_mode != KWB_NO_ABSORPTION;
   const bool nonlinear = P->BonA.count > 0;
@@ -550,6 +659,10 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     const size_t need = estimate_device_bytes(P);
     size_t free_b = 0, total_b = 0;
     CU(cudaMemGetInfo(&free_b, &total_b));
+    uint64_t reserved = 0, used = 0;  // blocks held idle by this context's pool are free here
+    CU(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    CU(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    if (reserved > used) free_b += (size_t)(reserved - used);
     if (need + (size_t)64 * 1024 * 1024 > free_b)
       return set_err(ctx, KWB_E_NOMEM, "simulation needs %.1f MB of device memory, %.1f MB free",
                      need / 1e6, free_b / 1e6);
@@ -574,24 +687,35 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   CU(cudaMemsetAsync(S->d_t0, 0, 8, st));
   h.t0 = S->d_t0;
 
-  // ---- medium (FP64 upload, FP32 on device)
-  double *stage = nullptr;
+  // ---- medium (FP64 upload, FP32 on device); the FP64 staging is set-up scratch only
+  TempBuf tmp(st, ctx->pool);
+  double *stage = nullptr, *stage2 = nullptr, *rm_in = nullptr;
   const bool need_stage = c_arr || r_arr || b_arr || P->p0.count;
-  if (need_stage) CU(M.alloc(&stage, nvox));
-  double *stage2 = nullptr;
-  if (nonlinear && b_arr && r_arr) CU(M.alloc(&stage2, nvox));
+  if (need_stage) CU(tmp.alloc(&stage, nvox));
+  if (nonlinear && b_arr && r_arr) CU(tmp.alloc(&stage2, nvox));
+  if (need_stage && P->row_major && D > 1) CU(tmp.alloc(&rm_in, nvox));
+  // one grid-shaped FP64 array into column-major device staging
+  auto upload_grid = [&](double *dst, const double *src) -> int {
+    if (!rm_in) return upload(ctx, dst, src, nvox * 8, st);
+    int r = upload(ctx, rm_in, src, nvox * 8, st);
+    if (r) return r;
+    CU(transpose_to_column_major(dst, rm_in, D, h.N, st));
+    return KWB_OK;
+  };
   if (c_arr) {
     float *c0sq;
     CU(M.alloc(&c0sq, nvox));
-    if ((rc = upload(ctx, stage, P->c0.data, nvox * 8, st))) return rc;
+    if ((rc = upload_grid(stage, P->c0.data))) return rc;
     CU(convert_f64_to_f32(c0sq, stage, nvox, 1, st));
     h.c0sq = c0sq;
   }
+  // rho0 stays staged in FP64 for the nonlinearity term (stage2 when B/A is an array too)
+  double *rho_stage = stage2 ? stage2 : stage;
   if (r_arr) {
     float *rho0;
     CU(M.alloc(&rho0, nvox));
-    if ((rc = upload(ctx, stage, P->rho0.data, nvox * 8, st))) return rc;
-    CU(convert_f64_to_f32(rho0, stage, nvox, 0, st));
+    if ((rc = upload_grid(rho_stage, P->rho0.data))) return rc;
+    CU(convert_f64_to_f32(rho0, rho_stage, nvox, 0, st));
     h.rho0 = rho0;
   }
   if (nonlinear) {
@@ -601,15 +725,13 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
       CU(M.alloc(&q, nvox));
       const double *bp = nullptr, *rp = nullptr;
       if (b_arr && r_arr) {
-        if ((rc = upload(ctx, stage, P->BonA.data, nvox * 8, st))) return rc;
-        if ((rc = upload(ctx, stage2, P->rho0.data, nvox * 8, st))) return rc;
+        if ((rc = upload_grid(stage, P->BonA.data))) return rc;
         bp = stage;
         rp = stage2;
       } else if (b_arr) {
-        if ((rc = upload(ctx, stage, P->BonA.data, nvox * 8, st))) return rc;
+        if ((rc = upload_grid(stage, P->BonA.data))) return rc;
         bp = stage;
       } else {
-        if ((rc = upload(ctx, stage, P->rho0.data, nvox * 8, st))) return rc;
         rp = stage;
       }
       CU(build_nlq(q, bp, b_arr, b_s, rp, r_arr, r_s, nvox, st));
@@ -675,7 +797,15 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     *dev_out = nullptr;
     if (!c_arr || n == 0) return KWB_OK;
     std::vector<double> c(n);
-    for (long long j = 0; j < n; ++j) c[j] = P->c0.data[idx[j]];
+    const long long Nx = h.N[0], Ny = h.N[1], Nz = h.N[2];
+    for (long long j = 0; j < n; ++j) {
+      long long k = idx[j];  // column-major linear index
+      if (P->row_major && D > 1) {
+        const long long x = k % Nx, y = (k / Nx) % Ny, z = k / (Nx * Ny);
+        k = D == 3 ? (x * Ny + y) * Nz + z : x * Ny + y;
+      }
+      c[j] = P->c0.data[k];
+    }
     double *dc;
     CU(M.alloc(&dc, n));
     if (int r = upload(ctx, dc, c.data(), n * 8, st)) return r;
@@ -842,7 +972,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
 
   // ---- p0 initialisation (first_order_steps.jl:58-191); skipped in time-reversal mode
   if (P->p0.count && !S->tr) {
-    if ((rc = upload(ctx, stage, P->p0.data, nvox * 8, st))) return rc;
+    if ((rc = upload_grid(stage, P->p0.data))) return rc;
     CU(convert_f64_to_f32(h.p, stage, nvox, 0, st));
     for (int a = 0; a < D; ++a) CU(launch_line_pass(S->d_sim, h, a, KWB_MODE_INIT, 0, st));
   }
@@ -939,8 +1069,6 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
   CU(cudaSetDevice(ctx->device));
   CU(cudaStreamSynchronize(S->stream));
   const double Ntd = (double)S->Nt_loop;
-  std::vector<float> f32;
-  std::vector<double> f64;
   for (size_t g = 0; g < S->groups.size(); ++g) {
     if (!out->groups) break;
     const GroupHost &G = S->groups[g];
@@ -963,14 +1091,17 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
     }
     const GroupDev &gd = G.dev;
     auto get32 = [&](const float *src, long long cnt, double *dst) -> int {
-      f32.resize(cnt);
-      CU(cudaMemcpy(f32.data(), src, cnt * 4, cudaMemcpyDeviceToHost));
-      for (long long i = 0; i < cnt; ++i) dst[i] = (double)f32[i];
-      return KWB_OK;
+      return read_f32_as_f64(ctx, S->stream, src, cnt, dst);
     };
     auto get64 = [&](const double *src, long long cnt, double *dst) -> int {
-      CU(cudaMemcpy(dst, src, cnt * 8, cudaMemcpyDeviceToHost));
+      CU(cudaMemcpyAsync(dst, src, cnt * 8, cudaMemcpyDeviceToHost, S->stream));
+      CU(cudaStreamSynchronize(S->stream));
       return KWB_OK;
+    };
+    auto rms = [&](double *a) {  // sqrt(sum / Nt), the reference's p_rms / u_rms
+      parallel_range(n, [a, Ntd](long long lo, long long hi) {
+        for (long long i = lo; i < hi; ++i) a[i] = std::sqrt(a[i] / Ntd);
+      });
     };
     int rc;
     if (want(KWB_REC_P) && (rc = get32(gd.ser_p, n * gd.nt_alloc, o.field[KWB_REC_P]))) return rc;
@@ -981,21 +1112,20 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
     if (want(KWB_REC_P_FINAL) && (rc = get32(gd.pfinal, n, o.field[KWB_REC_P_FINAL]))) return rc;
     if (want(KWB_REC_P_RMS)) {
       if ((rc = get64(gd.prms, n, o.field[KWB_REC_P_RMS]))) return rc;
-      for (long long i = 0; i < n; ++i) o.field[KWB_REC_P_RMS][i] = std::sqrt(o.field[KWB_REC_P_RMS][i] / Ntd);
+      rms(o.field[KWB_REC_P_RMS]);
     }
     if (want(KWB_REC_U_MAX) && (rc = get64(gd.umax, n, o.field[KWB_REC_U_MAX]))) return rc;
     if (want(KWB_REC_U_RMS)) {
       if ((rc = get64(gd.urms, n, o.field[KWB_REC_U_RMS]))) return rc;
-      for (long long i = 0; i < n; ++i) o.field[KWB_REC_U_RMS][i] = std::sqrt(o.field[KWB_REC_U_RMS][i] / Ntd);
+      rms(o.field[KWB_REC_U_RMS]);
     }
     if (want(KWB_REC_U_FINAL) && (rc = get64(gd.ufinal, n, o.field[KWB_REC_U_FINAL]))) return rc;
     if (want(KWB_REC_I_AVG) && (rc = get64(gd.iavg, n, o.field[KWB_REC_I_AVG]))) return rc;
     if (want(KWB_REC_I_MAX) && (rc = get64(gd.imax, n, o.field[KWB_REC_I_MAX]))) return rc;
   }
   if (S->tr && out->p_final_full) {
-    f32.resize(S->h.nvox);
-    CU(cudaMemcpy(f32.data(), S->h.p, S->h.nvox * 4, cudaMemcpyDeviceToHost));
-    for (long long i = 0; i < S->h.nvox; ++i) out->p_final_full[i] = (double)f32[i];
+    const int rc = read_f32_as_f64(ctx, S->stream, S->h.p, S->h.nvox, out->p_final_full);
+    if (rc) return rc;
   }
   return KWB_OK;
 }

@@ -175,6 +175,9 @@ cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const doub
                                  double c_ref, double dt, double c_sq_fold, int absorbing,
                                  double tau, double eta, double y, const int *slot_ky,
                                  cudaStream_t st);
+// Reorder a row-major grid array (NumPy order) into column-major (x fastest); ndim 2 or 3.
+cudaError_t transpose_to_column_major(double *out, const double *in, int ndim, const int N[3],
+                                      cudaStream_t st);
 cudaError_t convert_f64_to_f32(float *out, const double *in, long long n, int op,
                                cudaStream_t st);
 cudaError_t build_nlq(float *out, const double *bona, int bona_array, double bona_s,

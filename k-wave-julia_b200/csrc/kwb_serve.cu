@@ -68,7 +68,9 @@ struct KwbServer {
   std::unordered_map<uint64_t, Request *> all;
   uint64_t next_ticket = 1;
   bool stop = false;
-  int max_running = 64;
+  // A few concurrent simulations fill the GPU; more only split the L2 between their working
+  // sets and lengthen every request's latency.
+  int max_running = 8;
   int chunk = 32;
   size_t mem_cap = 0;  // 0: free device memory only
   size_t running_bytes = 0;

@@ -86,6 +86,23 @@ __global__ void k_build_eos_multiplier(float *M, float *M2, int Nx, int Ny, int 
   if (M2) M2[idx] = (float)(c_sq_fold * kappa * (eta * pow(kmag, y - 1.0)) * inv_total);
 }
 
+// Row-major (x slowest, f fastest: in[(x*Nm + m)*Nf + f]) to column-major
+// (out[x + Nx*(m + Nm*f)]) through a 32 x 32 shared tile, so that both sides are coalesced.
+// 3-D grids pass (Nx, Ny, Nz); 2-D grids (Nx, 1, Ny).
+__global__ void k_transpose_to_column_major(double *out, const double *in, int Nx, int Nm, int Nf) {
+  __shared__ double tile[32][33];
+  const int f0 = blockIdx.x * 32, x0 = blockIdx.y * 32, m = blockIdx.z;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int x = x0 + j, f = f0 + threadIdx.x;
+    if (x < Nx && f < Nf) tile[j][threadIdx.x] = in[((long long)x * Nm + m) * Nf + f];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int f = f0 + j, x = x0 + threadIdx.x;
+    if (x < Nx && f < Nf) out[x + (long long)Nx * (m + (long long)Nm * f)] = tile[threadIdx.x][j];
+  }
+}
+
 // op 0: copy, op 1: square
 __global__ void k_convert(float *out, const double *in, long long n, int op) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -141,6 +158,13 @@ cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const doub
   k_build_eos_multiplier<<<blocks(total, 256), 256, 0, st>>>(M, M2, N[0], N[1], N[2], d[0],
                                                              d[1], d[2], c_ref, dt, c_sq_fold,
                                                              absorbing, tau, eta, y, slot_ky);
+  return cudaGetLastError();
+}
+cudaError_t transpose_to_column_major(double *out, const double *in, int ndim, const int N[3],
+                                      cudaStream_t st) {
+  const int Nx = N[0], Nm = ndim == 3 ? N[1] : 1, Nf = ndim == 3 ? N[2] : N[1];
+  if (Nm > 65535) return cudaErrorInvalidValue;
+  k_transpose_to_column_major<<<dim3((Nf + 31) / 32, (Nx + 31) / 32, Nm), dim3(32, 8), 0, st>>>(out, in, Nx, Nm, Nf);
   return cudaGetLastError();
 }
 cudaError_t convert_f64_to_f32(float *out, const double *in, long long n, int op,

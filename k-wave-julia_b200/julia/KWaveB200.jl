@@ -73,6 +73,7 @@ struct KwbProblem
     groups::Ptr{KwbSensorGroup}
     progress::Ptr{Cvoid}
     progress_user::Ptr{Cvoid}
+    row_major::Int32  # 0: Julia arrays are column-major
 end
 struct KwbGroupSizes
     rows::NTuple{13,Int64}
@@ -198,7 +199,7 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
                        lossless ? 0.0 : Float64(medium.alpha_power), p0,
                        isempty(p_idx) ? C_NULL : pointer(p_idx), length(p_idx), Int32(Int(source.p_mode)), psig,
                        isempty(u_idx) ? C_NULL : pointer(u_idx), length(u_idx), Int32(Int(source.u_mode)), usig,
-                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL))
+                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL, Int32(0)))
     ctx = context()
     GC.@preserve keep begin
         sizes = Vector{KwbGroupSizes}(undef, max(length(groups), 1))

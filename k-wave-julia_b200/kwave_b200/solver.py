@@ -39,19 +39,32 @@ def _ptr_i(a: np.ndarray):
 
 
 def _flat(a, shape) -> np.ndarray:
-    """Column-major (Julia linear order) flattening of a grid-shaped array."""
+    """A grid-shaped array as a row-major (C-order) FP64 buffer, without a copy when it already
+    is one; the library reorders it to the reference's column-major layout on the device
+    (kwb_problem.row_major = 1).  A flat vector of the grid's size is read as column-major
+    (Julia linear order), as the reference would."""
     arr = np.asarray(a, dtype=np.float64)
     if arr.shape != tuple(shape):
         if arr.size == int(np.prod(shape)) and arr.ndim == 1:
-            return _f64(arr)
+            return _f64(arr.reshape(tuple(shape), order="F"))
         raise ValueError(f"array of shape {arr.shape} does not match the grid {tuple(shape)}")
-    return _f64(arr.ravel(order="F"))
+    return _f64(arr)
 
 
 def _findall(mask, shape) -> np.ndarray:
+    """findall(mask) - 1: sorted 0-based column-major linear indices of the True entries."""
     m = np.asarray(mask, dtype=bool)
     if m.shape != tuple(shape):
         raise ValueError(f"mask of shape {m.shape} does not match the grid {tuple(shape)}")
+    if m.ndim > 1 and 4 * int(np.count_nonzero(m)) <= m.size:
+        # sparse: coordinates in row-major order, then column-major linear index, sorted
+        coords = np.nonzero(m)
+        lin = np.zeros(coords[0].size, dtype=np.int64)
+        for ax in range(m.ndim - 1, -1, -1):
+            lin *= m.shape[ax]
+            lin += coords[ax]
+        lin.sort()
+        return lin
     return np.ascontiguousarray(np.flatnonzero(m.ravel(order="F")).astype(np.int64))
 
 
@@ -140,6 +153,7 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
         P.d[a] = kgrid.d[a] if a < D else 1.0
     P.dt = float(kgrid.dt)
     P.Nt = int(kgrid.Nt)
+    P.row_major = 1  # grid arrays go over as NumPy (row-major) buffers; see _flat
     if D == 1:
         if isinstance(pml_size, (tuple, list)) or isinstance(pml_alpha, (tuple, list)):
             raise TypeError("the 1D solver takes scalar pml_size and pml_alpha")
@@ -233,14 +247,15 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
         m = np.asarray(sen.mask)
         g = _lib.SensorGroup()
         if m.dtype == bool:
-            idx = b.arr(_findall(m, shape))
-            if idx.size == nvox and nvox > 0:
-                g.dense = 1
+            if m.shape == tuple(shape) and nvox > 0 and m.all():
+                g.dense = 1  # every voxel, in linear order: no index list
                 g.n_index = nvox
+                n_rows = nvox
             else:
+                idx = b.arr(_findall(m, shape))
                 g.index = _ptr_i(idx)
                 g.n_index = idx.size
-            n_rows = idx.size
+                n_rows = idx.size
         else:
             g.cartesian = 1
             g.n_index = int(m.shape[1])
@@ -545,7 +560,7 @@ def submit(kgrid, medium, source, sensor, *, pml_size=20, pml_alpha=2.0, smooth_
                                    smooth_p0=smooth_p0, extra_sensors=extra_sensors, context=context))
 
 
-def serving_config(max_running: int = 64, chunk_steps: int = 32, mem_cap_bytes: int = 0,
+def serving_config(max_running: int = 8, chunk_steps: int = 32, mem_cap_bytes: int = 0,
                    context: Optional[Context] = None):
     ctx = context or default_context()
     check(ctx.lib, ctx.handle, ctx.lib.kwb_serving_config(ctx.handle, max_running, chunk_steps, mem_cap_bytes))

@@ -199,6 +199,30 @@ def test_pressure_sources_2d_register_sizes(kb):
         assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
 
 
+def test_heterogeneous_sources_non_square_3d(kb):
+    """Row-major NumPy media on a non-square 3D grid (reordered on the device), with pressure
+    and velocity sources whose scaling reads c0 at the source points."""
+    from kwave_b200.workloads import Case, gaussian_random_field
+    shape = (24, 32, 20)
+    rng = np.random.default_rng(11)
+    c = gaussian_random_field(rng, shape, 2.0, 1450.0, 1600.0)
+    rho = gaussian_random_field(rng, shape, 2.0, 950.0, 1100.0)
+    dt = 0.3e-4 / 1600
+    t = np.arange(90) * dt
+    pm = np.zeros(shape, bool)
+    pm[8, 10:14, 9] = True
+    um = np.zeros(shape, bool)
+    um[15, 20, 6:9] = True
+    mask = np.zeros(shape, bool)
+    mask[4:20:3, 16, 10] = True
+    src = dict(p_mask=pm, p=np.vstack([np.sin(2 * math.pi * 1e6 * t)] * 4), u_mask=um,
+               ux=1e-3 * np.vstack([np.sin(2 * math.pi * 1.5e6 * t)] * 3))
+    case = Case("het_src", shape, (1e-4,) * 3, dt, 90,
+                dict(sound_speed=c, density=rho, alpha_coeff=0.5, alpha_power=1.5, alpha_mode="no_dispersion"),
+                src, dict(mask=mask, record=["p", "p_max"]), pml_size=4)
+    assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
+
+
 def test_velocity_recording_3d(kb):
     """test_solver_3d.jl:74-98 restated: 24^3 ball p0, record p, ux, uy, uz, u_max."""
     from kwave_b200.workloads import Case

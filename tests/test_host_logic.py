@@ -54,7 +54,9 @@ def test_build_problem_layout():
     # column-major (x fastest) linear indices, sorted, as findall returns
     idx = [P.p_index[i] for i in range(P.n_p_index)]
     assert idx == sorted([3 + n0 * 2, 7 + n0 * 2, 1 + n0 * 5])
-    assert P.c0.count == n0 * n1 and P.c0.data[3 + n0 * 2] == c[3, 2]
+    # grid arrays go over row-major (NumPy order, reordered on the device): (3, 2) at 3 * n1 + 2
+    assert P.row_major == 1
+    assert P.c0.count == n0 * n1 and P.c0.data[3 * n1 + 2] == c[3, 2]
     assert P.p_signal.n_rows == 3 and P.p_signal.n_cols == 2 and P.p_signal.data[1] == sig[1, 0]
     assert P.p_mode == 0 and P.alpha_mode == 2 and P.BonA.count == 1
     grp = P.groups[0]
@@ -106,3 +108,21 @@ def test_workloads_are_seeded_and_match_their_configs():
     sides = {W.c4_sim(i).N for i in range(8)}
     assert all(n in W.C4_SIDES for s in sides for n in s)
     assert W.smooth_sides(256, 300) == [256, 270, 288, 300]
+
+
+def test_findall_sparse_and_dense_paths_agree():
+    """Mask indices: the sparse path (row-major coordinates, sorted) and the column-major ravel
+    give the same findall(mask) - 1; an all-true sensor mask becomes a dense group."""
+    import kwave_b200 as kb
+    from kwave_b200.solver import _findall
+    rng = np.random.default_rng(7)
+    for shape in ((17, 9), (6, 11, 5)):
+        for frac in (0.05, 0.6):
+            m = rng.random(shape) < frac
+            ref = np.flatnonzero(m.ravel(order="F"))
+            assert np.array_equal(_findall(m, shape), ref)
+    g = kb.KWaveGrid(8, 1e-4, 6, 1e-4)
+    kb.make_time(g, 1500.0, t_end=1e-6)
+    b = kb.build_problem(g, kb.KWaveMedium(sound_speed=1500.0), kb.KWaveSource(p0=np.ones((8, 6))),
+                         kb.KWaveSensor(mask=np.ones((8, 6), bool), record=["p_max"]))
+    assert b.problem.groups[0].dense == 1 and b.problem.groups[0].n_index == 48
