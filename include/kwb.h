@@ -125,6 +125,11 @@ typedef struct kwb_problem {
    * fastest).  Row-major arrays are uploaded as they are and reordered on the device.  Index
    * lists (p_index, u_index, sensor indices) are column-major linear indices either way. */
   int32_t row_major;
+
+  /* 1: the axisymmetric solver, kspace_first_order_as (solver/axisymmetric.jl:26-227): ndim 2,
+   * x axial, y radial; the radial density update adds u_r / r to the divergence, r = |y_vec|
+   * with r = 0 replaced by dy/2.  Time-reversal data is not accepted with it. */
+  int32_t axisymmetric;
 } kwb_problem;
 
 /* Output sizes of one group: rows x cols per field, 0 x 0 when the field is not recorded. */

@@ -294,6 +294,10 @@ int validate_problem(kwb_ctx *ctx, const kwb_problem *P) {
   if (P->Nt == 0 || P->dt == 0)
     return set_err(ctx, KWB_E_INVALID, "Time array not set. Call make_time!(kgrid, sound_speed) before running.");
   if (P->Nt < 0 || !(P->dt > 0)) return set_err(ctx, KWB_E_INVALID, "Nt and dt must be positive");
+  if (P->axisymmetric && P->ndim != 2)
+    return set_err(ctx, KWB_E_INVALID, "the axisymmetric solver takes a 2D grid (x axial, y radial)");
+  if (P->axisymmetric && P->tr.data)
+    return set_err(ctx, KWB_E_INVALID, "time reversal is not part of the axisymmetric solver");
   for (int a = 0; a < P->ndim; ++a)
     if (P->pml_size[a] < 0) return set_err(ctx, KWB_E_INVALID, "pml_size must be >= 0");
   auto chk_field = [&](const kwb_field &f, const char *nm, bool optional) -> int {
@@ -763,6 +767,20 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     h.gneg[a] = gn;
     h.pml_def[a] = pd;
     h.pml_sg_def[a] = psd;
+  }
+  if (P->axisymmetric) {
+    // 1/r on the radial axis: r = |y_vec|, y_vec = ((0:Ny-1) - (Ny-1)/2) dy, r = 0 -> dy/2
+    // (grid.jl:137-139, axisymmetric.jl:100-103); FP64, rounded once
+    std::vector<float> ir(h.N[1]);
+    for (int j = 0; j < h.N[1]; ++j) {
+      double r = std::fabs((j - (h.N[1] - 1) / 2.0) * P->d[1]);
+      if (r == 0.0) r = P->d[1] / 2.0;
+      ir[j] = (float)(1.0 / r);
+    }
+    float *dir;
+    CU(M.alloc(&dir, h.N[1]));
+    if ((rc = upload(ctx, dir, ir.data(), ir.size() * sizeof(float), st))) return rc;
+    h.inv_r = dir;
   }
   {
     // 3-D y/z transforms in one cluster pass per kx plane (KWB_PLANE=0 keeps separate passes)

@@ -568,7 +568,13 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     const float2 nei = pair(-__ldg(ed + i));
     const float2 ncoef = rho0 ? pmul(pair(-S.dt), staged(st_r, i)) : pair(-S.dt_rho0_s);
     const float2 r0d = staged(st_p, i);
-    const float2 tr = pfma(ncoef, v[r], pfma(nei, r0d, r0d));
+    float2 du = v[r];
+    if (!CONTIG && axis == 1 && S.inv_r) {  // + u_r / r, the axisymmetric radial term (axisymmetric.jl:183)
+      // u_r as stored above by this thread: an ordinary (coherent) load, not the read-only path
+      const float2 ur = vb ? *reinterpret_cast<const float2 *>(ud + base + off(2 * l, i)) : make_float2(0.f, 0.f);
+      du = pfma(ur, pair(__ldg(S.inv_r + i)), du);
+    }
+    const float2 tr = pfma(ncoef, du, pfma(nei, r0d, r0d));
     v[r] = pfma(nei, tr, tr);
   }
   // pressure (mass) sources (first_order_steps.jl:619-640, 692-715)

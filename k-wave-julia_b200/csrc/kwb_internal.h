@@ -103,6 +103,10 @@ struct SimDev {
   const long long *t0;  // device step base (CUDA graph replays advance it)
 
   int fast;  // register-FFT kernels (kwb_fast.cu) for power-of-two lines: bit 0 line passes, bit 1 EOS passes
+
+  // axisymmetric solver: 1/r along the radial (y) axis, added as u_r / r to the y divergence;
+  // nullptr otherwise
+  const float *inv_r;
   // 3-D equation of state with the y/z transforms in one cluster pass per kx plane: the half
   // spectrum is then [z][kx][y] and M is [kx][k_z][slot] (slot: register order of the pass's y
   // transform, fast_plane_slot_ky)

@@ -250,8 +250,10 @@ __global__ void __launch_bounds__(KWB_THREADS)
         const long long ad = addr(c, i);
         const float coef = rho0 ? S.dt * rho0[ad] : S.dt_rho0_s;
         const float r0 = rd[ad];
+        float du = h ? g.y : g.x;
+        if (axis == 1 && S.inv_r) du = fmaf(ud[ad], S.inv_r[i], du);  // + u_r / r (axisymmetric.jl:183)
         float t1 = fmaf(-ei, r0, r0);
-        t1 = fmaf(-coef, h ? g.y : g.x, t1);
+        t1 = fmaf(-coef, du, t1);
         const float v = fmaf(-ei, t1, t1);
         rd[ad] = v;
         out[h] = v;

@@ -74,6 +74,7 @@ struct KwbProblem
     progress::Ptr{Cvoid}
     progress_user::Ptr{Cvoid}
     row_major::Int32  # 0: Julia arrays are column-major
+    axisymmetric::Int32
 end
 struct KwbGroupSizes
     rows::NTuple{13,Int64}
@@ -126,7 +127,7 @@ end
 const _ALPHA = Dict(:no_absorption => 0, :no_dispersion => 1, :stokes => 2)
 
 function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, data_cast,
-                progress_callback)
+                progress_callback; axisymmetric::Bool=false)
     (kgrid.Nt[] == 0 || kgrid.dt[] == 0) &&
         error("Time array not set. Call make_time!(kgrid, sound_speed) before running.")
     KWave.validate_record_fields(sensor)
@@ -142,7 +143,7 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
     if !lossless && !(medium.alpha_coeff isa Real)
         error("array alpha_coeff is not supported")          # T(absorb_tau) raises in the reference
     end
-    tr = KWave.is_time_reversal(sensor)
+    tr = KWave.is_time_reversal(sensor) && !axisymmetric  # the axisymmetric solver ignores TR data
     p0 = KwbField(C_NULL, 0)
     if KWave.has_p0(source) && !tr
         q = Float64.(Array(source.p0))
@@ -199,7 +200,7 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
                        lossless ? 0.0 : Float64(medium.alpha_power), p0,
                        isempty(p_idx) ? C_NULL : pointer(p_idx), length(p_idx), Int32(Int(source.p_mode)), psig,
                        isempty(u_idx) ? C_NULL : pointer(u_idx), length(u_idx), Int32(Int(source.u_mode)), usig,
-                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL, Int32(0)))
+                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL, Int32(0), Int32(axisymmetric)))
     ctx = context()
     GC.@preserve keep begin
         sizes = Vector{KwbGroupSizes}(undef, max(length(groups), 1))
@@ -249,6 +250,23 @@ function kspace_first_order(kgrid::KWave.AbstractKWaveGrid, medium::KWave.KWaveM
                             progress_callback=nothing, show_progress::Bool=true) where {T<:AbstractFloat}
     save_to_disk === nothing || error("save_to_disk (HDF5 input files) is not supported by KWaveB200")
     return _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, T, progress_callback)
+end
+
+"""
+    kspace_first_order_as(kgrid, medium, source, sensor; kwargs...) -> SimulationOutput
+
+Same arguments and output as `KWave.kspace_first_order_as` (2D grid, x axial, y radial); the time
+loop runs on the GPU.
+"""
+function kspace_first_order_as(kgrid::KWave.KWaveGrid2D, medium::KWave.KWaveMedium,
+                               source::KWave.KWaveSource, sensor::KWave.KWaveSensor;
+                               pml_inside::Bool=true, pml_size=20, pml_alpha=2.0,
+                               smooth_p0::Bool=true, smooth_c0::Bool=false, smooth_rho0::Bool=false,
+                               data_cast::Type{T}=Float64, plot_sim::Bool=false,
+                               plot_layout::Symbol=:default, plot_scale=:auto,
+                               record_movie=nothing, progress_callback=nothing) where {T<:AbstractFloat}
+    return _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, T, progress_callback;
+                  axisymmetric=true)
 end
 
 end # module

@@ -11,7 +11,7 @@ from .core import (Additive, AdditiveNoCorrection, Dirichlet, KWaveGrid, KWaveMe
                    make_time, neper2db, smooth, tone_burst, validate_record_fields)
 from ._lib import KWaveB200Error, LIB_PATH, load_library
 from .solver import (Context, Prepared, Request, Simulation, prepare, solve_prepared, submit_prepared, build_problem, default_context, estimate_device_bytes,
-                     kspace_first_order, serving_config, serving_stats, shard_jobs, solve_batch, submit)
+                     kspace_first_order, kspace_first_order_as, serving_config, serving_stats, shard_jobs, solve_batch, submit)
 
 make_time_ = make_time  # `make_time!` in the reference
 
@@ -21,7 +21,7 @@ __all__ = [
     "get_optimal_pml_size", "get_pml", "make_ball", "make_circle", "make_disc", "make_line",
     "make_time", "make_time_", "neper2db", "smooth", "tone_burst", "validate_record_fields",
     "KWaveB200Error", "LIB_PATH", "load_library", "Context", "Simulation", "build_problem",
-    "default_context", "kspace_first_order", "Request", "estimate_device_bytes", "serving_config",
+    "default_context", "kspace_first_order", "kspace_first_order_as", "Request", "estimate_device_bytes", "serving_config",
     "serving_stats", "shard_jobs", "solve_batch", "submit", "Prepared", "prepare", "solve_prepared",
     "submit_prepared",
 ]

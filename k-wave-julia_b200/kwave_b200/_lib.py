@@ -72,7 +72,7 @@ class Problem(C.Structure):
         ("tr", Signal),
         ("n_groups", C.c_int32), ("groups", C.POINTER(SensorGroup)),
         ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
-        ("row_major", C.c_int32),
+        ("row_major", C.c_int32), ("axisymmetric", C.c_int32),
     ]
 
 

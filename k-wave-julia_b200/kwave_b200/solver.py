@@ -132,7 +132,7 @@ class _Built:
 
 def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
                   pml_size=20, pml_alpha=2.0, smooth_p0: bool = True, data_cast=np.float64,
-                  progress_callback=None, extra_sensors=()) -> _Built:
+                  progress_callback=None, extra_sensors=(), axisymmetric: bool = False) -> _Built:
     """Normalise the reference's arguments into a kwb_problem (first_order.jl:311-441, 529-669).
 
     ``extra_sensors`` (not in the reference API) adds further sensor groups -- (mask, record)
@@ -154,6 +154,7 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
     P.dt = float(kgrid.dt)
     P.Nt = int(kgrid.Nt)
     P.row_major = 1  # grid arrays go over as NumPy (row-major) buffers; see _flat
+    P.axisymmetric = 1 if axisymmetric else 0
     if D == 1:
         if isinstance(pml_size, (tuple, list)) or isinstance(pml_alpha, (tuple, list)):
             raise TypeError("the 1D solver takes scalar pml_size and pml_alpha")
@@ -196,7 +197,7 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
         P.alpha_coeff = float(medium.alpha_coeff)
         P.alpha_power = float(medium.alpha_power)
 
-    tr = sensor.is_time_reversal()
+    tr = sensor.is_time_reversal() and not axisymmetric  # the axisymmetric solver ignores TR data
     if source.p0 is not None and not tr:
         p0 = np.asarray(source.p0, dtype=np.float64)
         if p0.shape != tuple(shape):
@@ -398,6 +399,28 @@ def kspace_first_order(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSourc
     if sensor.is_time_reversal():
         kgrid.Nt = int(Nt_loop)  # the reference mutates kgrid.Nt[] (first_order.jl:430-431)
     return _collect(b, arrays, pfull, sensor, kgrid, Nt_loop)
+
+
+def kspace_first_order_as(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
+                          sensor: KWaveSensor, *, pml_inside: bool = True, pml_size=20,
+                          pml_alpha=2.0, smooth_p0: bool = True, smooth_c0: bool = False,
+                          smooth_rho0: bool = False, data_cast=np.float64, plot_sim: bool = False,
+                          plot_layout: str = "default", plot_scale="auto", record_movie=None,
+                          progress_callback=None, context: Optional[Context] = None) -> SimulationOutput:
+    """Axisymmetric solve on a 2D grid, x axial and y radial (``kspace_first_order_as``,
+    solver/axisymmetric.jl:26-227): the 2D time step with u_r / r added to the radial divergence.
+    Same arguments and output as the reference; like it, time-reversal data on the sensor is not
+    used (the sensor records as usual)."""
+    if kgrid.ndim != 2:
+        raise TypeError("MethodError: kspace_first_order_as takes a KWaveGrid2D (x axial, y radial)")
+    ctx = context or default_context()
+    b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
+                      smooth_p0=smooth_p0, data_cast=data_cast, progress_callback=progress_callback,
+                      axisymmetric=True)
+    with ctx.lock:
+        O, outs, arrays, pfull = _alloc_outputs(ctx, b, kgrid)
+        check(ctx.lib, ctx.handle, ctx.lib.kwb_solve(ctx.handle, C.byref(b.problem), C.byref(O)))
+    return _collect(b, arrays, pfull, sensor, kgrid, int(b.problem.Nt))
 
 
 class Simulation:

@@ -607,10 +607,31 @@ def apply_frequency_response(sensor_data, sensor: KWaveSensor, grid: KWaveGrid):
 # kspace_first_order (solver/first_order.jl:92-728)
 # ---------------------------------------------------------------------------------------------
 
+def kspace_first_order_as(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
+                          pml_size=20, pml_alpha=2.0, smooth_p0: bool = True, dtype=np.float64,
+                          max_steps: Optional[int] = None, progress_callback=None) -> dict:
+    """Restates ``kspace_first_order_as`` (solver/axisymmetric.jl:26-227): the 2D solver with x
+    axial and y radial, whose radial density update carries the cylindrical term u_r / r
+    (axisymmetric.jl:183, 186), r = |y_vec| with r = 0 replaced by dy/2 (:100-103).  Time-reversal
+    data is not used by that solver (it records the sensor as usual)."""
+    if grid.ndim != 2:
+        raise TypeError("kspace_first_order_as takes a 2D grid (x axial, y radial)")
+    return kspace_first_order(grid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
+                              smooth_p0=smooth_p0, dtype=dtype, max_steps=max_steps,
+                              progress_callback=progress_callback, _axisymmetric=True)
+
+
+def radial_distance(grid: KWaveGrid) -> np.ndarray:
+    """axisymmetric.jl:100-103 -- r = |y_vec|, with r = 0 replaced by dy / 2."""
+    r = np.abs(make_spatial_vec(grid.N[1], grid.d[1]))
+    r[r == 0] = grid.d[1] / 2
+    return r
+
+
 def kspace_first_order(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
                        pml_size=20, pml_alpha=2.0, smooth_p0: bool = True, dtype=np.float64,
                        max_steps: Optional[int] = None, progress_callback=None,
-                       extra_sensors=()) -> dict:
+                       extra_sensors=(), _axisymmetric: bool = False) -> dict:
     """Restates ``kspace_first_order`` for 1D/2D/3D grids; returns the sensor-data dict.
 
     Oracle-only conveniences (not in the reference): ``max_steps`` stops the time loop early
@@ -678,8 +699,9 @@ def kspace_first_order(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource
         es = es if isinstance(es, KWaveSensor) else KWaveSensor(**es)
         extras.append((es, _create_sensor_data(es, Nt), findall(es.mask)))
 
-    tr = sensor.time_reversal_boundary_data is not None
+    tr = sensor.time_reversal_boundary_data is not None and not _axisymmetric
     tr_data = None
+    r_row = radial_distance(grid).reshape(1, -1).astype(dtype) if _axisymmetric else None
     if tr:
         tr_data = np.asarray(sensor.time_reversal_boundary_data, dtype=np.float64)
         Nt = tr_data.shape[1]
@@ -740,6 +762,8 @@ def kspace_first_order(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource
         # STEP 4-5: divergence, density update with PML
         for d in range(D):
             g = spectral_gradient(u[d], k_ops[d], s_neg[d], plans, d, dtype)
+            if r_row is not None and d == 1:
+                g = g + u[1] / r_row  # axisymmetric.jl:183, 186: div u gains u_r / r
             rho[d][...] = pml[d] * (pml[d] * rho[d] - dt * rho0 * g)
         # STEP 6: pressure sources
         if has_p_src:

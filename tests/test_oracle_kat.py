@@ -269,3 +269,54 @@ def test_per_mode_recurrence_matches_stepping(shape):
         p = np.real(np.fft.ifftn(P))
         stepped = out["p"][:, n - 1].reshape(shape, order="F")
         assert np.max(np.abs(stepped - p)) <= 1e-10 * np.max(np.abs(p)), n
+
+
+def test_axisymmetric_basic_run():  # test_axisymmetric.jl:2-27
+    Nx, Nr, dx = 64, 32, 1e-4
+    g = K.KWaveGrid(Nx, dx, Nr, dx)
+    med = K.KWaveMedium(sound_speed=1500.0, density=1000.0)
+    K.make_time(g, 1500.0, t_end=2e-6)
+    i = np.arange(1, Nx + 1)[:, None]
+    j = np.arange(1, Nr + 1)[None, :]
+    p0 = np.exp(-(((i - Nx // 2) * dx) ** 2 + ((j - Nr // 2) * dx) ** 2) / (5 * dx) ** 2)
+    mask = np.zeros((Nx, Nr), bool)
+    mask[Nx // 2 - 1, :] = True
+    out = K.kspace_first_order_as(g, med, K.KWaveSource(p0=p0), K.KWaveSensor(mask=mask, record=["p"]))
+    assert "p" in out and out["p"].shape == (Nr, g.Nt)
+    assert np.all(np.isfinite(out["p"]))
+
+
+def test_axisymmetric_with_absorption():  # test_axisymmetric.jl:29-50
+    Nx = Nr = 64
+    dx = 1e-4
+    g = K.KWaveGrid(Nx, dx, Nr, dx)
+    med = K.KWaveMedium(sound_speed=1500.0, density=1000.0, alpha_coeff=0.5, alpha_power=1.5,
+                        alpha_mode="no_dispersion")
+    K.make_time(g, 1500.0, t_end=1e-6)
+    p0 = np.zeros((Nx, Nr))
+    p0[Nx // 2 - 1, Nr // 2 - 1] = 1.0
+    mask = np.zeros((Nx, Nr), bool)
+    mask[Nx // 2 - 1, 0] = True
+    out = K.kspace_first_order_as(g, med, K.KWaveSource(p0=p0), K.KWaveSensor(mask=mask, record=["p_max"]),
+                                  pml_size=10)
+    assert "p_max" in out and np.isfinite(out["p_max"]).all()
+
+
+def test_axisymmetric_radial_term():
+    """r = |y_vec| never vanishes for an even radial size and is dy/2 at the axis for an odd one
+    (axisymmetric.jl:100-103); the u_r / r term changes the solution against the plain 2D solver."""
+    g = K.KWaveGrid(32, 1e-4, 16, 1e-4)
+    r = K.radial_distance(g)
+    assert np.allclose(r, np.abs((np.arange(16) - 7.5) * 1e-4)) and r.min() > 0
+    g3 = K.KWaveGrid(32, 1e-4, 15, 1e-4)
+    r3 = K.radial_distance(g3)
+    assert r3[7] == 0.5e-4 and np.isclose(r3[0], 7e-4)
+    K.make_time(g, 1500.0, t_end=1e-6)
+    p0 = np.zeros((32, 16))
+    p0[15, 6:10] = 1.0
+    mask = np.ones((32, 16), bool)
+    med = K.KWaveMedium(sound_speed=1500.0, density=1000.0)
+    a = K.kspace_first_order_as(g, med, K.KWaveSource(p0=p0), K.KWaveSensor(mask=mask, record=["p_final"]), pml_size=4)
+    b = K.kspace_first_order(g, med, K.KWaveSource(p0=p0), K.KWaveSensor(mask=mask, record=["p_final"]), pml_size=4)
+    rel = np.linalg.norm(a["p_final"] - b["p_final"]) / np.linalg.norm(b["p_final"])
+    assert rel > 1e-3
