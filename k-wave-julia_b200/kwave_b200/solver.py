@@ -340,8 +340,12 @@ def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt
     return out
 
 
+_FILTER_ROWS = 4096  # sensor rows transformed at once by the post-loop filters (bounds memory)
+
+
 def apply_sensor_directivity(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
-    """first_order_steps.jl:836-873 -- per-sensor sinc(k a sin(theta)/2) filter of p (host, FP64)."""
+    """first_order_steps.jl:836-873 -- per-sensor sinc(k a sin(theta)/2) filter of p (host, FP64),
+    all sensors with a non-zero angle at once (rows with angle 0 are left as they are)."""
     if sensor.directivity_angle is None or sensor.directivity_size is None or "p" not in data:
         return
     p = data["p"]
@@ -349,27 +353,28 @@ def apply_sensor_directivity(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
     freqs = np.fft.fftfreq(Nt, kgrid.dt)
     dmin = kgrid.d[0] if kgrid.ndim == 1 else min(kgrid.d)
     ang = np.asarray(sensor.directivity_angle, dtype=np.float64)
+    th = np.full(n, float(ang)) if ang.ndim == 0 else ang.ravel()[:n]
     kval = 2 * math.pi * np.abs(freqs) / dmin
-    for j in range(n):
-        th = float(ang) if ang.ndim == 0 else float(ang.ravel()[j])
-        if abs(th) <= 1.4901161193847656e-08 * abs(th) or th == 0.0:
-            continue
-        arg = kval * sensor.directivity_size * math.sin(th) / 2
+    rows = np.flatnonzero(th != 0.0)  # `angle ≈ 0` with default tolerances holds only for 0
+    for lo in range(0, rows.size, _FILTER_ROWS):
+        r = rows[lo: lo + _FILTER_ROWS]
+        arg = kval[None, :] * sensor.directivity_size * np.sin(th[r])[:, None] / 2
         with np.errstate(invalid="ignore", divide="ignore"):
             filt = np.where(arg == 0, 1.0, np.sin(arg) / np.where(arg == 0, 1.0, arg))
-        p[j, :] = np.real(np.fft.ifft(np.fft.fft(p[j, :]) * filt))
+        p[r, :] = np.real(np.fft.ifft(np.fft.fft(p[r, :], axis=1) * filt, axis=1))
 
 
 def apply_frequency_response(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
-    """first_order_steps.jl:880-910 -- Gaussian band-pass of p (host, FP64)."""
+    """first_order_steps.jl:880-910 -- Gaussian band-pass of p (host, FP64), all sensors at once."""
     if sensor.frequency_response is None or "p" not in data:
         return
     fc, bw = sensor.frequency_response
     p = data["p"]
     n, Nt = p.shape
     resp = np.exp(-((np.abs(np.fft.fftfreq(Nt, kgrid.dt)) - fc) ** 2) / (2 * bw ** 2))
-    for j in range(n):
-        p[j, :] = np.real(np.fft.ifft(np.fft.fft(p[j, :]) * resp))
+    for lo in range(0, n, _FILTER_ROWS):
+        p[lo: lo + _FILTER_ROWS, :] = np.real(np.fft.ifft(np.fft.fft(p[lo: lo + _FILTER_ROWS, :], axis=1) * resp,
+                                                          axis=1))
 
 
 def kspace_first_order(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
