@@ -171,7 +171,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def batch_bench(ctx, n_sims=64, max_running=8, one_at_a_time=True):
+def batch_bench(ctx, n_sims=64, max_running=64, one_at_a_time=True):
     """Config 4: n mixed-size 2D simulations, batched (continuous batching, all submitted at once)
     against one-at-a-time blocking solves of the same prepared problems.  Sims/s is measured
     from the first submission to the last completion (host wall clock, device work inside)."""
@@ -209,7 +209,7 @@ def batch_bench(ctx, n_sims=64, max_running=8, one_at_a_time=True):
     return res
 
 
-def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800), max_running=8, one_at_a_time=True):
+def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800), max_running=64, one_at_a_time=True):
     """Config 5: Poisson arrivals (mean rate 200/s) of mixed 2D/3D requests; latency is arrival to
     completion.  The comparison serves the same arrivals one at a time with blocking solves."""
     import threading

@@ -225,10 +225,14 @@ typedef struct kwb_serving_stats {
   int64_t queued, running, running_bytes;
 } kwb_serving_stats;
 
-/* Scheduler limits: at most `max_running` admitted simulations (default 8), `chunk_steps` time
+/* Scheduler limits: at most `max_running` admitted simulations (default 64), `chunk_steps` time
  * steps per launch (default 32), and (if > 0) at most `mem_cap_bytes` of modelled device memory
  * in use. */
 int kwb_serving_config(kwb_ctx *ctx, int32_t max_running, int32_t chunk_steps, int64_t mem_cap_bytes);
+/* Admission by size: a queued request starts while the running simulations hold at most
+ * `voxels` grid points in total (default 4 Mi), or when none is running; 0 removes the limit.
+ * No counterpart in the reference (scheduling of many kspace_first_order calls). */
+int kwb_serving_voxel_budget(kwb_ctx *ctx, int64_t voxels);
 int kwb_submit(kwb_ctx *ctx, const kwb_problem *problem, kwb_outputs *outputs, uint64_t *ticket);
 /* *done = 1 once the request has completed (successfully or not). */
 int kwb_poll(kwb_ctx *ctx, uint64_t ticket, int32_t *done);

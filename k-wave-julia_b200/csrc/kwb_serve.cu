@@ -51,6 +51,7 @@ struct Request {
   cudaEvent_t ev = nullptr;
   bool inflight = false;
   size_t bytes = 0;
+  long long voxels = 0;
   int64_t t_submit = 0, t_start = 0, t_end = 0;
   std::string err;
 };
@@ -68,9 +69,13 @@ struct KwbServer {
   std::unordered_map<uint64_t, Request *> all;
   uint64_t next_ticket = 1;
   bool stop = false;
-  // A few concurrent simulations fill the GPU; more only split the L2 between their working
+  int max_running = 64;
+  // Admission by size: a request starts while the running simulations hold at most this many
+  // voxels (or when nothing runs).  Small grids cannot fill the GPU alone, so many run together;
+  // large ones run a few at a time, since more would only split the L2 between their working
   // sets and lengthen every request's latency.
-  int max_running = 8;
+  long long voxel_budget = 4LL << 20;
+  long long running_voxels = 0;
   int chunk = 32;
   size_t mem_cap = 0;  // 0: free device memory only
   size_t running_bytes = 0;
@@ -92,6 +97,7 @@ struct KwbServer {
     if (r->sim) kwb_sim_destroy(r->sim);
     r->sim = nullptr;
     running_bytes -= std::min(running_bytes, r->bytes);
+    running_voxels -= std::min(running_voxels, r->voxels);
   }
 
   // Admit queued requests while slots and memory allow.  Called with `mu` held; drops it around
@@ -106,6 +112,9 @@ struct KwbServer {
         changed = true;
         continue;
       }
+      long long vox = 1;
+      for (int a = 0; a < r->P->ndim; ++a) vox *= r->P->N[a];
+      if (!running.empty() && voxel_budget > 0 && running_voxels + vox > voxel_budget) break;
       const size_t need = estimate_device_bytes(r->P);
       if (mem_cap && running_bytes + need > mem_cap) {
         if (running.empty()) {  // can never fit under the cap
@@ -143,6 +152,8 @@ struct KwbServer {
       r->ev = ev;
       r->bytes = need;
       running_bytes += need;
+      r->voxels = vox;
+      running_voxels += vox;
       r->state = 1;
       r->t_start = now_ns();
       running.push_back(r);
@@ -280,6 +291,15 @@ void kwb_server_shutdown(kwb_ctx *ctx) {
 }
 
 extern "C" {
+
+int kwb_serving_voxel_budget(kwb_ctx *ctx, int64_t voxels) {
+  if (!ctx || voxels < 0) return KWB_E_INVALID;
+  KwbServer *s = server_of(ctx, kwb_ctx_server_slot(ctx));
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->voxel_budget = voxels;
+  s->cv_work.notify_all();
+  return KWB_OK;
+}
 
 int kwb_serving_config(kwb_ctx *ctx, int32_t max_running, int32_t chunk_steps, int64_t mem_cap_bytes) {
   if (!ctx || max_running < 1 || chunk_steps < 1 || mem_cap_bytes < 0) return KWB_E_INVALID;

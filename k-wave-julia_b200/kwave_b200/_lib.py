@@ -162,6 +162,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         lib.kwb_estimate_device_bytes.argtypes = [vp, C.POINTER(Problem), C.POINTER(C.c_int64)]
         lib.kwb_serving_config.restype = C.c_int
         lib.kwb_serving_config.argtypes = [vp, C.c_int32, C.c_int32, C.c_int64]
+        lib.kwb_serving_voxel_budget.restype = C.c_int
+        lib.kwb_serving_voxel_budget.argtypes = [vp, C.c_int64]
         lib.kwb_submit.restype = C.c_int
         lib.kwb_submit.argtypes = [vp, C.POINTER(Problem), C.POINTER(Outputs), C.POINTER(C.c_uint64)]
         lib.kwb_poll.restype = C.c_int

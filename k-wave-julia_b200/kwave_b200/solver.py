@@ -588,10 +588,14 @@ def submit(kgrid, medium, source, sensor, *, pml_size=20, pml_alpha=2.0, smooth_
                                    smooth_p0=smooth_p0, extra_sensors=extra_sensors, context=context))
 
 
-def serving_config(max_running: int = 8, chunk_steps: int = 32, mem_cap_bytes: int = 0,
-                   context: Optional[Context] = None):
+def serving_config(max_running: int = 64, chunk_steps: int = 32, mem_cap_bytes: int = 0,
+                   context: Optional[Context] = None, voxel_budget: Optional[int] = None):
+    """Scheduler limits (kwb_serving_config); ``voxel_budget`` (kwb_serving_voxel_budget) caps
+    the grid points of the running simulations together (default 4 Mi; 0 = no cap)."""
     ctx = context or default_context()
     check(ctx.lib, ctx.handle, ctx.lib.kwb_serving_config(ctx.handle, max_running, chunk_steps, mem_cap_bytes))
+    if voxel_budget is not None:
+        check(ctx.lib, ctx.handle, ctx.lib.kwb_serving_voxel_budget(ctx.handle, int(voxel_budget)))
 
 
 def serving_stats(context: Optional[Context] = None) -> dict:
