@@ -359,6 +359,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <class F, bool CONTIG, int LT, int MINB, bool XEOS>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_line_fast(const __grid_constant__ SimDev S, int axis, int mode, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int RP = G + 1, LP = F::LP;
   constexpr int L = LT;  // complex lines per tile
@@ -673,6 +674,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_fwd_fast(const __grid_constant__ SimDev S, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
@@ -761,6 +763,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_inv_fast(const __grid_constant__ SimDev S, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
@@ -887,6 +890,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 template <class F, int LT, int MINB>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_spec_fast(const __grid_constant__ SimDev S, int axis, int op, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, L = LT;
   extern __shared__ float4 smem_raw[];
@@ -993,6 +997,7 @@ __device__ __forceinline__ unsigned cluster_rank() {
 template <class FY, class FZ, int CL>
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 2)
     k_plane_fast(const __grid_constant__ SimDev S, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int NY = FY::N, NZ = FZ::N, RZ = NZ / CL, CY = NY / CL;
   constexpr int LY = KWB_PLANE_THREADS / FY::G, LZ = KWB_PLANE_THREADS / FZ::G;
   static_assert(RZ == 2 * LY && CY % LZ == 0 && RZ == FZ::G, "plane tiling");
@@ -1185,13 +1190,12 @@ static void line_go(const SimDev *d_sim, const SimDev &h, int axis, int mode, lo
     using F = typename P::template F<true>;
     const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
     if (h.fuse_xeos && mode == KWB_MODE_STEP)
-      k_line_fast<F, true, LT, P::MINB, true><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(h, axis, mode, s);
+      kwb_launch(k_line_fast<F, true, LT, P::MINB, true>, grid, LT * F::G, pline_smem<F>(LT), st, h, axis, mode, s);
     else
-      k_line_fast<F, true, LT, P::MINB, false><<<grid, LT * F::G, pline_smem<F>(LT), st>>>(h, axis, mode, s);
+      kwb_launch(k_line_fast<F, true, LT, P::MINB, false>, grid, LT * F::G, pline_smem<F>(LT), st, h, axis, mode, s);
   } else {
     using F = typename P::template F<false>;
-    k_line_fast<F, false, LT, P::MINB, false><<<cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G,
-                                         pline_smem<F>(LT), st>>>(h, axis, mode, s);
+    kwb_launch(k_line_fast<F, false, LT, P::MINB, false>, cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G, pline_smem<F>(LT), st, h, axis, mode, s);
   }
 }
 
@@ -1247,11 +1251,11 @@ static void eos_go(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, 
   using F = typename P::template F<true>;
   const int grid = cdiv(h.N[1], 2 * LT) * h.N[2];
   if (h.plane) {
-    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
-    else k_eos_inv_fast<F, LT, P::MINB, true><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
+    if (fwd) kwb_launch(k_eos_fwd_fast<F, LT, P::MINB, true>, grid, LT * F::G, eos_smem<F>(LT), st, h, s);
+    else kwb_launch(k_eos_inv_fast<F, LT, P::MINB, true>, grid, LT * F::G, eos_smem<F>(LT), st, h, s);
   } else {
-    if (fwd) k_eos_fwd_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
-    else k_eos_inv_fast<F, LT, P::MINB, false><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, s);
+    if (fwd) kwb_launch(k_eos_fwd_fast<F, LT, P::MINB, false>, grid, LT * F::G, eos_smem<F>(LT), st, h, s);
+    else kwb_launch(k_eos_inv_fast<F, LT, P::MINB, false>, grid, LT * F::G, eos_smem<F>(LT), st, h, s);
   }
 }
 
@@ -1274,7 +1278,7 @@ static void spec_go(const SimDev *d_sim, const SimDev &h, int axis, int op, long
   using P = LinePolicy<N>;
   using F = typename P::template F<false>;
   const int grid = cdiv(h.n1, LT) * (axis == 1 ? h.N[2] : h.N[1]);
-  k_spec_fast<F, LT, P::MINB><<<grid, LT * F::G, eos_smem<F>(LT), st>>>(h, axis, op, s);
+  kwb_launch(k_spec_fast<F, LT, P::MINB>, grid, LT * F::G, eos_smem<F>(LT), st, h, axis, op, s);
 }
 
 template <int N>
@@ -1336,8 +1340,7 @@ void fast_plane_slot_ky(int Ny, int *ky) {
   for (int s = 0; s < Ny; ++s) ky[s] = F::k_of(s % F::G, s / F::G);
 }
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
-  fast::k_plane_fast<fast::PlaneFY, fast::PlaneFZ, fast::kPlaneCL>
-      <<<h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st>>>(h, s);
+  kwb_launch(fast::k_plane_fast<fast::PlaneFY, fast::PlaneFZ, fast::kPlaneCL>, h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st, h, s);
   return cudaGetLastError();
 }
 

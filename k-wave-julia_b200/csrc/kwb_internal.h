@@ -10,6 +10,7 @@
 //     multipliers i k e^{+-i k d/2}/N, PML deficits 1 - pml, and the EOS multiplier
 //     M = [c^2] kappa (1 + nabla1) / (Nx Ny Nz) in the half-spectrum shape.
 #pragma once
+#include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -17,6 +18,18 @@
 #define KWB_THREADS 256
 #define KWB_MAX_N 4096
 #define KWB_CHUNK_STEPS 32  // time steps per replayed CUDA graph
+
+// Programmatic dependent launch between the kernels of a time step.  Each step kernel is
+// launched with kwb_launch, so its blocks may be dispatched while its predecessor finishes; its
+// first statement waits for the predecessor to complete (every block, before any early return,
+// so completion stays ordered along the stream), and it then lets its own successor be
+// dispatched (which needs every block of this kernel to be resident already, so it never holds
+// back this kernel's blocks).
+#define KWB_STEP_KERNEL_PROLOGUE()                                  \
+  do {                                                              \
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");            \
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); \
+  } while (0)
 
 struct FftPlan {
   int n;
@@ -121,6 +134,23 @@ struct SimDev {
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
 };
+
+// Launch a step kernel with programmatic stream serialization (see KWB_STEP_KERNEL_PROLOGUE).
+template <typename... K, typename... A>
+inline cudaError_t kwb_launch(void (*kern)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              A &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 // Sensor group on the device.
 struct GroupDev {

@@ -87,6 +87,7 @@ __device__ __forceinline__ void load_twiddles(float2 *tw, const float2 *g, int N
 template <bool CONTIG>
 __global__ void __launch_bounds__(KWB_THREADS)
     k_line_pass(const SimDev *__restrict__ sims, int axis, int mode, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   extern __shared__ float4 smem_raw[];
   float2 *smem = reinterpret_cast<float2 *>(smem_raw);
   const SimDev &S = sims[0];
@@ -303,6 +304,7 @@ __device__ __forceinline__ float eos_effective(const SimDev &S, long long v, flo
 
 __global__ void __launch_bounds__(KWB_THREADS)
     k_eos_x_fwd(const SimDev *__restrict__ sims, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   extern __shared__ float4 smem_raw[];
   float2 *smem = reinterpret_cast<float2 *>(smem_raw);
   const SimDev &S = sims[0];
@@ -368,6 +370,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
 
 __global__ void __launch_bounds__(KWB_THREADS)
     k_eos_x_inv(const SimDev *__restrict__ sims, long long step_s, int mul_x) {
+  KWB_STEP_KERNEL_PROLOGUE();
   extern __shared__ float4 smem_raw[];
   float2 *smem = reinterpret_cast<float2 *>(smem_raw);
   const SimDev &S = sims[0];
@@ -437,6 +440,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
 // y- or z-direction FFTs of the half spectrum (complex columns kx0..kx0+L-1)
 __global__ void __launch_bounds__(KWB_THREADS)
     k_spec_pass(const SimDev *__restrict__ sims, int axis, int op, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   extern __shared__ float4 smem_raw[];
   float2 *smem = reinterpret_cast<float2 *>(smem_raw);
   const SimDev &S = sims[0];
@@ -511,6 +515,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
 // ------------------------------------------------------------------------------------------
 
 __global__ void k_tr_inject(const SimDev *__restrict__ sims, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   const SimDev &S = sims[0];
   const long long t = step_index(S, step_s);
   if (t >= S.Nt) return;
@@ -524,6 +529,7 @@ __global__ void k_tr_inject(const SimDev *__restrict__ sims, long long step_s) {
 
 __global__ void k_sensor_gather(const SimDev *__restrict__ sims, const GroupDev *__restrict__ gp,
                                 long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
   const SimDev &S = sims[0];
   const long long t = step_index(S, step_s);
   if (t >= S.Nt) return;
@@ -564,6 +570,7 @@ __global__ void k_sensor_gather(const SimDev *__restrict__ sims, const GroupDev 
 }
 
 __global__ void k_advance_t0(long long *t0, long long k) {
+  KWB_STEP_KERNEL_PROLOGUE();
   if (threadIdx.x == 0 && blockIdx.x == 0) *t0 += k;
 }
 
@@ -600,10 +607,10 @@ cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int
   int tiles;
   if (axis == 0) {
     tiles = cdiv(h.N[1], 2 * L) * h.N[2];
-    k_line_pass<true><<<tiles, KWB_THREADS, sm, st>>>(d_sim, axis, mode, step_s);
+    kwb_launch(k_line_pass<true>, tiles, KWB_THREADS, sm, st, d_sim, axis, mode, step_s);
   } else {
     tiles = cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]);
-    k_line_pass<false><<<tiles, KWB_THREADS, sm, st>>>(d_sim, axis, mode, step_s);
+    kwb_launch(k_line_pass<false>, tiles, KWB_THREADS, sm, st, d_sim, axis, mode, step_s);
   }
   return cudaGetLastError();
 }
@@ -614,7 +621,7 @@ cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long ste
   const int L = h.L_eosx;
   const size_t sm = spec_pass_smem(h.N[0], L, h.dispersion);
   const int tiles = cdiv(h.N[1], 2 * L) * h.N[2];
-  k_eos_x_fwd<<<tiles, KWB_THREADS, sm, st>>>(d_sim, step_s);
+  kwb_launch(k_eos_x_fwd, tiles, KWB_THREADS, sm, st, d_sim, step_s);
   return cudaGetLastError();
 }
 
@@ -624,7 +631,7 @@ cudaError_t launch_eos_x_inv(const SimDev *d_sim, const SimDev &h, long long ste
   const int L = h.L_eosx;
   const size_t sm = line_pass_smem(h.N[0], L);
   const int tiles = cdiv(h.N[1], 2 * L) * h.N[2];
-  k_eos_x_inv<<<tiles, KWB_THREADS, sm, st>>>(d_sim, step_s, h.ndim == 1 ? 1 : 0);
+  kwb_launch(k_eos_x_inv, tiles, KWB_THREADS, sm, st, d_sim, step_s, h.ndim == 1 ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -634,14 +641,14 @@ cudaError_t launch_spec_pass(const SimDev *d_sim, const SimDev &h, int axis, int
   const int L = h.L_spec[axis];
   const size_t sm = spec_pass_smem(h.N[axis], L, h.dispersion && op != KWB_SPEC_INV);
   const int tiles = cdiv(h.n1, L) * (axis == 1 ? h.N[2] : h.N[1]);
-  k_spec_pass<<<tiles, KWB_THREADS, sm, st>>>(d_sim, axis, op, step_s);
+  kwb_launch(k_spec_pass, tiles, KWB_THREADS, sm, st, d_sim, axis, op, step_s);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tr_inject(const SimDev *d_sim, const SimDev &h, long long step_s,
                              cudaStream_t st) {
   if (h.n_tr <= 0) return cudaSuccess;
-  k_tr_inject<<<cdiv(h.n_tr, 256), 256, 0, st>>>(d_sim, step_s);
+  kwb_launch(k_tr_inject, cdiv(h.n_tr, 256), 256, 0, st, d_sim, step_s);
   return cudaGetLastError();
 }
 
@@ -649,7 +656,7 @@ cudaError_t launch_sensor_gather(const SimDev *d_sim, const SimDev &h, const Gro
                                  long long n, long long step_s, cudaStream_t st) {
   (void)h;
   if (n <= 0) return cudaSuccess;
-  k_sensor_gather<<<cdiv(n, 256), 256, 0, st>>>(d_sim, d_group, step_s);
+  kwb_launch(k_sensor_gather, cdiv(n, 256), 256, 0, st, d_sim, d_group, step_s);
   return cudaGetLastError();
 }
 
@@ -671,7 +678,7 @@ cudaError_t prime_attributes(const SimDev &h) {
 }
 
 cudaError_t launch_advance_t0(long long *t0, long long k, cudaStream_t st) {
-  k_advance_t0<<<1, 32, 0, st>>>(t0, k);
+  kwb_launch(k_advance_t0, 1, 32, 0, st, t0, k);
   return cudaGetLastError();
 }
 
