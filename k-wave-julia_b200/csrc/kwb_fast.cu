@@ -359,7 +359,6 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <class F, bool CONTIG, int LT, int MINB, bool XEOS>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_line_fast(const __grid_constant__ SimDev S, int axis, int mode, long long step_s) {
-  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int RP = G + 1, LP = F::LP;
   constexpr int L = LT;  // complex lines per tile
@@ -368,6 +367,9 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   float2 *tw2 = sm + L * LP;
   float2 *gp2 = tw2 + F::TW;
   float2 *gn2 = gp2 + E * RP;
+  // the tables are written once at set-up: built before waiting on the previous kernel
+  build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
+  KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (mode == KWB_MODE_STEP && t >= S.Nt) return;
   const int tid = threadIdx.x;
@@ -462,7 +464,6 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   stage(st_p, S.p);
   if (rho0) stage(st_r, rho0);
   else cp_async_commit();
-  build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
   float2 *xs = sm + l * LP;
   float *__restrict__ ud = S.u[axis];
   cp_async_wait<1>();  // the p tile has landed (rho0 may still be in flight)
@@ -674,12 +675,14 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_fwd_fast(const __grid_constant__ SimDev S, long long step_s) {
-  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
+  // the twiddles are written once at set-up: built before waiting on the previous kernel
+  F::build_tw(tw2, S.tw[0]);
+  KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;
   const int tid = threadIdx.x, tt = tid % G, l = tid / G;
@@ -689,7 +692,6 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   const int cnt = min(rows, Ny - y0);
   const long long base = ((long long)z * Ny + y0) * N;
   const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
-  F::build_tw(tw2, S.tw[0]);
   // One field at a time over all E positions: each loop issues 2E independent loads, so
   // every thread keeps many requests in flight (the sum, nonlinearity and c^2 follow).
   auto ld = [&](const float *__restrict__ f, int i) -> float2 {
@@ -763,12 +765,14 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 template <class F, int LT, int MINB, bool PLANE>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_inv_fast(const __grid_constant__ SimDev S, long long step_s) {
-  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
+  // the twiddles are written once at set-up: built before waiting on the previous kernel
+  F::build_tw(tw2, S.tw[0]);
+  KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;
   const int tid = threadIdx.x, tt = tid % G, l = tid / G;
@@ -778,7 +782,6 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   const int cnt = min(rows, Ny - y0);
   const long long base = ((long long)z * Ny + y0) * N;
   const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
-  F::build_tw(tw2, S.tw[0]);
   float2 *xs = sm + l * LP;
   const int n1 = S.n1;
   if (PLANE) {
@@ -890,12 +893,14 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 template <class F, int LT, int MINB>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_spec_fast(const __grid_constant__ SimDev S, int axis, int op, long long step_s) {
-  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, L = LT;
   extern __shared__ float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
+  // the twiddles are written once at set-up: built before waiting on the previous kernel
+  F::build_tw(tw2, S.tw[axis]);
+  KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;
   const int tid = threadIdx.x, l = tid % L, tt = tid / L;
@@ -912,7 +917,6 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     base = (long long)o * n1 + k0 + l;
     stride = (long long)n1 * Ny;
   }
-  F::build_tw(tw2, S.tw[axis]);
   float2 *xs = sm + l * LP;
   float2 *__restrict__ spec = S.spec;
   float2 v[E];
@@ -997,7 +1001,6 @@ __device__ __forceinline__ unsigned cluster_rank() {
 template <class FY, class FZ, int CL>
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 2)
     k_plane_fast(const __grid_constant__ SimDev S, long long step_s) {
-  KWB_STEP_KERNEL_PROLOGUE();
   constexpr int NY = FY::N, NZ = FZ::N, RZ = NZ / CL, CY = NY / CL;
   constexpr int LY = KWB_PLANE_THREADS / FY::G, LZ = KWB_PLANE_THREADS / FZ::G;
   static_assert(RZ == 2 * LY && CY % LZ == 0 && RZ == FZ::G, "plane tiling");
@@ -1007,6 +1010,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 
   float2 *xsb = data + RZ * NY;
   float2 *twy = xsb + XS;
   float2 *twz = twy + FY::TW;
+  // the twiddles are written once at set-up: built before waiting on the previous kernel
+  FY::build_tw(twy, S.tw[1]);
+  FZ::build_tw(twz, S.tw[2]);
+  KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;  // uniform over the cluster
   const unsigned rank = cluster_rank();
@@ -1024,8 +1031,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 
     }
     cp_async_commit();
   }
-  FY::build_tw(twy, S.tw[1]);
-  FZ::build_tw(twz, S.tw[2]);
 
   // 1. forward along y
   {
