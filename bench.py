@@ -172,7 +172,7 @@ def run_reference(args, world, rank):
 
 
 def batch_bench(ctx, n_sims=64, max_running=64, one_at_a_time=True):
-    """Config 4: n mixed-size 2D simulations, batched (continuous batching, all submitted at once)
+    """Batch workload: n mixed-size 2D simulations, batched (continuous batching, all submitted at once)
     against one-at-a-time blocking solves of the same prepared problems.  Sims/s is measured
     from the first submission to the last completion (host wall clock, device work inside)."""
     import numpy as np
@@ -210,7 +210,7 @@ def batch_bench(ctx, n_sims=64, max_running=64, one_at_a_time=True):
 
 
 def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800), max_running=64, one_at_a_time=True):
-    """Config 5: Poisson arrivals (mean rate 200/s) of mixed 2D/3D requests; latency is arrival to
+    """Serving workload: Poisson arrivals (mean rate 200/s) of mixed 2D/3D requests; latency is arrival to
     completion.  The comparison serves the same arrivals one at a time with blocking solves."""
     import threading
     import numpy as np
@@ -279,8 +279,8 @@ def main():
     ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-batch", action="store_true", help="skip the batched (config 4) measurement")
-    ap.add_argument("--no-serve", action="store_true", help="skip the serving (config 5) measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-size 2D measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the Poisson serving measurement")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":

@@ -1351,16 +1351,6 @@ cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaSt
 
 bool fast_size(int N) { return N == 64 || N == 128 || N == 256 || N == 512 || N == 1024; }
 
-#define KWB_FAST_SWITCH(N, FN, ARGS)                                   \
-  switch (N) {                                                         \
-    case 64: return fast::FN<8, 8> ARGS;                               \
-    case 128: return fast::FN<16, 8> ARGS;                             \
-    case 256: return fast::FN<16, 16> ARGS;                            \
-    case 512: return fast::FN<32, 16> ARGS;                            \
-    case 1024: return fast::FN<32, 32> ARGS;                           \
-    default: return cudaErrorInvalidValue;                             \
-  }
-
 #define KWB_LINE_SWITCH(N, FN, ARGS)       \
   switch (N) {                             \
     case 64: return fast::FN<64> ARGS;     \

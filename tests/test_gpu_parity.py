@@ -31,7 +31,7 @@ def wl():
 
 
 def test_c1_homogeneous_disc_source(kb, wl):
-    """Config 1: 128^2 homogeneous lossless, 81-point disc p-source, 228-point circle sensor."""
+    """128^2 homogeneous lossless medium, 81-point disc p-source, 228-point circle sensor, 689 steps."""
     case = wl.c1()
     assert case.Nt == 689
     rep = {}
@@ -40,7 +40,7 @@ def test_c1_homogeneous_disc_source(kb, wl):
 
 
 def test_c2_reduced_heterogeneous_absorbing(kb, wl):
-    """Config 2 at 128^2 / 400 steps: heterogeneous c/rho, y=1.5 :stokes, smoothed line p0."""
+    """Heterogeneous absorbing 2D workload reduced to 128^2 / 400 steps: c/rho fields, y=1.5 :stokes, smoothed line p0."""
     case = wl.c2(n=128, Nt=400, record=("p", "p_max", "p_rms", "p_min", "p_final"))
     rep = {}
     assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX, report=rep)
@@ -48,7 +48,7 @@ def test_c2_reduced_heterogeneous_absorbing(kb, wl):
 
 
 def test_c3_reduced_nonlinear_piston(kb, wl):
-    """Config 3 at 48^3 / 150 steps: heterogeneous c/rho/BonA, y=1.1, ux piston, plane p + volume p_max."""
+    """Nonlinear absorbing 3D workload reduced to 48^3 / 150 steps: heterogeneous c/rho/BonA, y=1.1, ux piston, plane p + volume p_max."""
     case = wl.c3(n=48, Nt=150, piston=8, pml=6)
     g = run_gpu(case)
     r = run_oracle(case)
@@ -59,7 +59,7 @@ def test_c3_reduced_nonlinear_piston(kb, wl):
 
 
 def test_c2_full_size_prefix_and_properties(kb, wl):
-    """Config 2 at full size: 100-step prefix against the oracle, then the full 2000-step run."""
+    """The 512^2 x 2000-step heterogeneous workload: 100-step prefix against the oracle, then the full run."""
     case = wl.c2(n=512, Nt=2000)
     pre = wl.c2(n=512, Nt=100, record=("p_max", "p_rms"))
     assert_parity(run_gpu(pre), run_oracle(pre), TOL_L2, TOL_MAX)
@@ -73,7 +73,7 @@ def test_c2_full_size_prefix_and_properties(kb, wl):
 
 
 def test_c3_full_size_prefix_and_properties(kb, wl):
-    """Config 3 at full size: 4-step prefix against the oracle, then 300 steps of properties."""
+    """The 256^3 nonlinear absorbing workload: 4-step prefix against the oracle, then 300 steps of properties."""
     pre = wl.c3(n=256, Nt=4)
     g = run_gpu(pre)
     r = run_oracle(pre)

@@ -104,7 +104,7 @@ def test_make_time():  # test_grid.jl:65-84
     assert g.t_array[1] == pytest.approx(dt)
     dt2, Nt2 = K.make_time(g, 1500.0, t_end=1e-5)
     assert Nt2 == math.ceil(1e-5 / dt2) + 1
-    # config 1: dt = 2e-8, Nt = 689
+    # the 128^2 disc-source workload: dt = 2e-8, Nt = 689
     g = grid2(128)
     assert K.make_time(g, 1500.0, t_end=1.14 * math.sqrt(2) * 128e-4 / 1500) == (2e-8, 689) or \
         (abs(g.dt - 2e-8) < 1e-20 and g.Nt == 689)
