@@ -892,6 +892,12 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
 
   // ---- sensor groups
   S->groups.resize(P->n_groups);
+  // Pressure-only groups can be recorded by the fast x C2R pass as it writes p: one dense group
+  // (every voxel) and one sparse group (through a per-x-line index of its points).
+  const unsigned ponly = (1u << KWB_REC_P) | (1u << KWB_REC_P_MAX) | (1u << KWB_REC_P_MIN) |
+                         (1u << KWB_REC_P_RMS) | (1u << KWB_REC_P_FINAL);
+  const bool fast_inv = (h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0]);
+  bool sparse_taken = false;
   for (int g = 0; g < P->n_groups; ++g) {
     GroupHost &G = S->groups[g];
     G.spec = P->groups[g];
@@ -934,9 +940,32 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (m & (1u << KWB_REC_U_FINAL)) { CU(M.alloc(&gd.ufinal, G.n)); if ((rc = fill_f64(ctx, gd.ufinal, G.n, 0.0, st))) return rc; }
     if (m & (1u << KWB_REC_I_AVG)) { CU(M.alloc(&gd.iavg, G.n)); if ((rc = fill_f64(ctx, gd.iavg, G.n, 0.0, st))) return rc; }
     if (m & (1u << KWB_REC_I_MAX)) { CU(M.alloc(&gd.imax, G.n)); if ((rc = fill_f64(ctx, gd.imax, G.n, -INFINITY, st))) return rc; }
+    if (fast_inv && !S->tr && !in.dense && !sparse_taken && !(m & ~ponly)) {
+      // per-x-line index of the points: the sorted column-major indices are sorted by line, then x
+      const long long Nx = h.N[0], nlines = (long long)h.N[1] * h.N[2];
+      std::vector<int> ptr(nlines + 1, 0);
+      std::vector<int2> ent(G.n);
+      for (long long j = 0; j < G.n; ++j) {
+        const long long v = in.index[j];
+        ptr[v / Nx + 1]++;
+        ent[j] = make_int2((int)(v % Nx), (int)j);
+      }
+      for (long long k = 0; k < nlines; ++k) ptr[k + 1] += ptr[k];
+      int *dptr;
+      int2 *dent;
+      CU(M.alloc(&dptr, ptr.size()));
+      CU(M.alloc(&dent, ent.size()));
+      if ((rc = upload(ctx, dptr, ptr.data(), ptr.size() * sizeof(int), st))) return rc;
+      if ((rc = upload(ctx, dent, ent.data(), ent.size() * sizeof(int2), st))) return rc;
+      gd.line_ptr = dptr;
+      gd.line_ent = dent;
+      G.fused = true;
+      sparse_taken = true;
+    }
     CU(M.alloc(&G.d_dev, 1));
     if ((rc = upload(ctx, G.d_dev, &gd, sizeof(GroupDev), st))) return rc;
     CU(cudaStreamSynchronize(st));
+    if (G.fused) h.sparse_p = G.d_dev;
   }
 
   // ---- time reversal data: p / (D c^2) at group 0's points
@@ -971,9 +1000,6 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
 
   // ---- a dense pressure-only sensor group is updated inside the fast x C2R pass
   {
-    const unsigned ponly = (1u << KWB_REC_P) | (1u << KWB_REC_P_MAX) | (1u << KWB_REC_P_MIN) |
-                           (1u << KWB_REC_P_RMS) | (1u << KWB_REC_P_FINAL);
-    const bool fast_inv = (h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0]);
     for (auto &G : S->groups) {
       if (!fast_inv || G.spec.cartesian || !G.dev.dense || G.n == 0 || (G.dev.mask & ~ponly)) continue;
       h.dense_p = G.d_dev;

@@ -888,6 +888,33 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     }
     if ((gm & (1u << 4)) && t == S.Nt - 1) put(gd->pfinal + ra);
   }
+  // sparse pressure sensor (record_sensor_data!, first_order_steps.jl:732-752): this thread's
+  // p values go to its line's exchange buffer (x order, the two rows as one pair), then the
+  // points on the line pair are recorded from there through the group's per-x-line index
+  const GroupDev *gs = S.sparse_p;
+  if (gs) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) xs[tt + G * r] = v[r];
+    F::sync();
+    const unsigned sm_ = gs->mask;
+    const bool last = (t == S.Nt - 1);
+    const int line0 = z * Ny + y0 + 2 * l;
+    for (int c = 0; c < 2; ++c) {
+      if (!(c ? vb : va)) continue;
+      const int q0 = gs->line_ptr[line0 + c], q1 = gs->line_ptr[line0 + c + 1];
+      for (int q = q0 + tt; q < q1; q += G) {
+        const int2 e = gs->line_ent[q];
+        const float2 pp = xs[e.x];
+        const float pv = c ? pp.y : pp.x;
+        const long long j = e.y;
+        if (sm_ & (1u << 0)) gs->ser_p[t * gs->n + j] = pv;
+        if (sm_ & (1u << 1)) gs->pmax[j] = fmaxf(gs->pmax[j], pv);
+        if (sm_ & (1u << 2)) gs->pmin[j] = fminf(gs->pmin[j], pv);
+        if (sm_ & (1u << 3)) gs->prms[j] += (double)gs->cnt_prms * ((double)pv * (double)pv);
+        if ((sm_ & (1u << 4)) && last) gs->pfinal[j] = pv;
+      }
+    }
+  }
 }
 
 template <class F, int LT, int MINB>

@@ -130,6 +130,9 @@ struct SimDev {
   // A dense (every-voxel) sensor group recording only pressure fields, updated by the x C2R
   // pass as it writes p (no separate gather); nullptr when there is none.
   const struct GroupDev *dense_p;
+  // A sparse pressure-only sensor group also recorded by that pass (per-x-line index in
+  // GroupDev::line_ptr / line_ent); nullptr when there is none.
+  const struct GroupDev *sparse_p;
 
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
@@ -165,6 +168,10 @@ struct GroupDev {
   float *pmax, *pmin, *pfinal;
   double *prms;
   double *umax, *urms, *ufinal, *iavg, *imax;
+  // sparse groups recorded by the x C2R pass: points of x-line (y + Ny z) are entries
+  // line_ptr[line] .. line_ptr[line+1]-1 of line_ent = {x, j}, sorted by x
+  const int *line_ptr;
+  const int2 *line_ent;
 };
 
 // Kernel launchers (kwb_kernels.cu).
