@@ -99,6 +99,7 @@ struct LineFFT {
   static constexpr int E = E_, G = G_;
   static constexpr int N = E * G, J = E / G, RP = G + 1, LP = E * RP + 1;
   static_assert(E % G == 0, "G must divide E");
+  static constexpr bool WARP_SYNC = WARP;  // one line per warp: exchanges need only __syncwarp
   __device__ __forceinline__ static void sync() {
     if (WARP) __syncwarp();
     else __syncthreads();
@@ -194,6 +195,7 @@ struct LineFFT3 {
     const int p0 = t * P3, q1 = p0 / B, mb = p0 - q1 * B + idx / A;  // B is a multiple of P3
     return nat3(q1, mb, idx % A);
   }
+  static constexpr bool WARP_SYNC = WARP;  // one line per warp: exchanges need only __syncwarp
   __device__ __forceinline__ static void sync() {
     if (WARP) __syncwarp();
     else __syncthreads();
@@ -893,15 +895,24 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // points on the line pair are recorded from there through the group's per-x-line index
   const GroupDev *gs = S.sparse_p;
   if (gs) {
+    const int line0 = z * Ny + y0 + 2 * l;
+    const int qa = va ? gs->line_ptr[line0] : 0;
+    const int qb = va ? gs->line_ptr[line0 + 1] : 0;
+    const int qc = vb ? gs->line_ptr[line0 + 2] : qb;
+    // most lines hold no point: skip the exchange unless some line of the group (the warp for
+    // one-warp lines, else the block) does
+    bool any = qc > qa;
+    if (F::WARP_SYNC) any = __any_sync(0xffffffffu, any);
+    else any = __syncthreads_or(any);
+    if (!any) return;
 #pragma unroll
     for (int r = 0; r < E; ++r) xs[tt + G * r] = v[r];
     F::sync();
     const unsigned sm_ = gs->mask;
     const bool last = (t == S.Nt - 1);
-    const int line0 = z * Ny + y0 + 2 * l;
     for (int c = 0; c < 2; ++c) {
       if (!(c ? vb : va)) continue;
-      const int q0 = gs->line_ptr[line0 + c], q1 = gs->line_ptr[line0 + c + 1];
+      const int q0 = c ? qb : qa, q1 = c ? qc : qb;
       for (int q = q0 + tt; q < q1; q += G) {
         const int2 e = gs->line_ent[q];
         const float2 pp = xs[e.x];
