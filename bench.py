@@ -31,7 +31,7 @@ sys.path.insert(0, os.path.join(ROOT, "k-wave-julia_b200"))
 # `bench.py --steps 4 --warmup 3 --no-e2e --no-cpu --no-batch --no-serve` on a B200.  Reads
 # equal the algorithmic bytes; writes land lower because part of each launch's output is still
 # in L2 when the launch ends.
-NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 710.85e6}
+NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 710.25e6}
 
 SPM_WORDS = {"c3": 33.0, "c2": 26.0, "c1": 15.01}
 UNIT = "Gvoxel-steps/s"
