@@ -133,6 +133,91 @@ def barrier(pg, local):
         barrier_max(pg, local, 0.0)
 
 
+def cufft_comparator(case, steps=20, warmup=3):
+    """A comparator timed beside the product, not part of it: the reference's time step written
+    with library FFTs -- torch.fft (cuFFT), FP32, on the GPU.  Every spectral derivative is a full
+    N-D real FFT pair, as the reference computes it (spectral_gradient!, fft_utils.jl:126-182):
+    4D + 2 transforms per step (D gradients of p, D divergences of u, the equation of state), with
+    the same PML, staggered densities, nonlinearity, k-space multiplier and velocity source."""
+    import numpy as np
+    import torch
+    from kwave_b200.core import db2neper, get_pml
+    from kwave_b200.solver import _findall
+    dev = torch.device("cuda", torch.cuda.current_device())
+    N = tuple(case.N)
+    D = len(N)
+    dt = case.dt
+    f32 = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float32), device=dev)
+    med = case.medium
+    c0 = np.asarray(med["sound_speed"], dtype=np.float64)
+    r0 = np.asarray(med["density"], dtype=np.float64)
+    c0sq, rho0 = f32(c0 ** 2), f32(r0)
+    Q = f32(np.asarray(med["BonA"], np.float64) / (2 * r0)) if med.get("BonA") is not None else None
+    rho_sg = [0.5 * (rho0 + torch.roll(rho0, -1, dims=a)) for a in range(D)]
+
+    def along(v, a):
+        sh = [1] * D
+        sh[a] = -1
+        return v.reshape(sh)
+
+    pml = [along(f32(get_pml(N[a], case.d[a], case.pml_size, case.pml_alpha, dt)), a) for a in range(D)]
+    pml_sg = [along(f32(get_pml(N[a], case.d[a], case.pml_size, case.pml_alpha, dt, staggered=True)), a)
+              for a in range(D)]
+    # wavenumbers in torch.fft.rfftn's layout (the last axis halved)
+    kv = [2 * np.pi * (np.fft.rfftfreq(N[a], case.d[a]) if a == D - 1 else np.fft.fftfreq(N[a], case.d[a]))
+          for a in range(D)]
+    op = lambda a, sgn: along(torch.as_tensor((1j * kv[a] * np.exp(sgn * 1j * kv[a] * case.d[a] / 2))
+                                              .astype(np.complex64), device=dev), a)
+    ops_pos = [op(a, 1) for a in range(D)]
+    ops_neg = [op(a, -1) for a in range(D)]
+    kk = np.sqrt(sum(g ** 2 for g in np.meshgrid(*kv, indexing="ij")))
+    c_ref = float(np.mean(c0))
+    y = float(med.get("alpha_power") or 1.0)
+    tau = -2 * db2neper(float(med.get("alpha_coeff") or 0.0), y) * c_ref ** (y - 1)
+    M = torch.as_tensor((np.sinc(c_ref * kk * dt / 2 / np.pi) * (1 + tau * kk ** y)).astype(np.float32), device=dev)
+    p = torch.zeros(N, device=dev)
+    u = [torch.zeros(N, device=dev) for _ in range(D)]
+    rho = [torch.zeros(N, device=dev) for _ in range(D)]
+    uidx = usig = None
+    if "u_mask" in case.source and case.source.get("ux") is not None:
+        lin = _findall(case.source["u_mask"], N)  # column-major order, the signal's row order
+        co = np.unravel_index(lin, N, order="F")
+        uidx = torch.as_tensor(np.ravel_multi_index(co, N), device=dev)  # the same points, C order
+        usig = f32(case.source["ux"])
+
+    def step(t):
+        for a in range(D):
+            g = torch.fft.irfftn(torch.fft.rfftn(p) * ops_pos[a], s=N)
+            u[a] = pml_sg[a] * (pml_sg[a] * u[a] - dt / rho_sg[a] * g)
+        if uidx is not None:
+            u[0].view(-1)[uidx] += usig[:, min(t, usig.shape[1] - 1)]
+        for a in range(D):
+            g = torch.fft.irfftn(torch.fft.rfftn(u[a]) * ops_neg[a], s=N)
+            rho[a] = pml[a] * (pml[a] * rho[a] - dt * rho0 * g)
+        rt = sum(rho[1:], rho[0])
+        if Q is not None:
+            rt = rt * (1 + Q * rt)
+        p.copy_(torch.fft.irfftn(torch.fft.rfftn(c0sq * rt) * M, s=N))
+
+    for t in range(warmup):
+        step(t)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for t in range(steps):
+        step(warmup + t)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"what": "the reference's time step with torch.fft (cuFFT) full N-D real FFT pairs, FP32, "
+                   f"{4 * D + 2} transforms per step, eager", "ms_per_step": ms,
+           "value": float(np.prod(N)) / (ms / 1e3) / 1e9, "unit": UNIT, "steps": steps, "warmup": warmup,
+           "finite": bool(torch.isfinite(p).all().item())}
+    del p, u, rho, M, rho_sg, pml, pml_sg, ops_pos, ops_neg, c0sq, rho0, Q
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_baseline(case_name, budget_s=20.0):
     """The FP64 oracle (restatement of the reference algorithm) on the host cores, a bounded
     number of time steps of the same workload; returns voxel-steps/s and the sample."""
@@ -281,6 +366,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-size 2D measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the Poisson serving measurement")
+    ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT-based comparator")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -343,6 +429,10 @@ def main():
     batch = None if args.no_batch else batch_bench(ctx)
     serve = None if args.no_serve else serving_bench(ctx)
 
+    comparators = None
+    if rank == 0 and world == 1 and not args.no_cufft:
+        comparators = {"cufft_reference_step": cufft_comparator(case)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, steps, el, cores = cpu_baseline(args.config)
@@ -371,6 +461,7 @@ def main():
             "batch": batch,
             "serving": serve,
             "cpu_baseline": cpu,
+            "comparators": comparators,
             "clocks": clk.summary(),
             "gpu_launches": info["launches_per_step"] * K + (K // 32),
         }
