@@ -807,3 +807,225 @@ def kspace_first_order(grid: KWaveGrid, medium: KWaveMedium, source: KWaveSource
     apply_sensor_directivity(sensor_data, sensor, grid)
     apply_frequency_response(sensor_data, sensor, grid)
     return sensor_data
+
+
+# ---------------------------------------------------------------------------------------------
+# pstd_elastic_2d / pstd_elastic_3d (solver/elastic.jl:133-588)
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class ElasticMedium:
+    """solver/elastic.jl:22-48."""
+    sound_speed_compression: Any
+    sound_speed_shear: Any
+    density: Any = 1000.0
+    alpha_coeff_compression: Any = None
+    alpha_coeff_shear: Any = None
+    alpha_power: Optional[float] = None
+
+
+@dataclass
+class ElasticSource:
+    """solver/elastic.jl:57-104: stress sources on s_mask, velocity sources on u_mask, p0."""
+    s_mask: Any = None
+    sxx: Any = None
+    syy: Any = None
+    szz: Any = None
+    sxy: Any = None
+    sxz: Any = None
+    syz: Any = None
+    s_mode: int = ADDITIVE
+    u_mask: Any = None
+    ux: Any = None
+    uy: Any = None
+    uz: Any = None
+    u_mode: int = ADDITIVE
+    p0: Any = None
+
+
+# stress components in the order (xx, yy, zz, xy, xz, yz); sigma_{dj} of axes d, j
+STRESS_NAMES = ("sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+
+def stress_slot(d: int, j: int) -> int:
+    """Slot of sigma_{dj} in STRESS_NAMES (symmetric in d, j)."""
+    return d if d == j else 2 + d + j
+
+
+def elastic_lame(medium: ElasticMedium):
+    """solver/elastic.jl:168-174, 419-423: lambda = rho (cp^2 - 2 cs^2), mu = rho cs^2.
+
+    With a scalar density the reference writes ``rho0 * (cp^2 - 2 * cs^2)``, which for an array
+    ``cp`` or ``cs`` is a matrix power (or a MethodError in 3D), not an element-wise square; that
+    combination is rejected here rather than reproduced."""
+    cp, cs, rho0 = medium.sound_speed_compression, medium.sound_speed_shear, medium.density
+    if _is_scalar(rho0):
+        if not (_is_scalar(cp) and _is_scalar(cs)):
+            raise TypeError("a scalar density with array wave speeds is evaluated as a matrix power "
+                            "(cp^2) by the reference (solver/elastic.jl:169); give the density as an array")
+        return float(rho0) * (float(cp) ** 2 - 2 * float(cs) ** 2), float(rho0) * float(cs) ** 2
+    rho0 = np.asarray(rho0, np.float64)
+    cp = cp if _is_scalar(cp) else np.asarray(cp, np.float64)
+    cs = cs if _is_scalar(cs) else np.asarray(cs, np.float64)
+    return rho0 * (np.square(cp) - 2 * np.square(cs)), rho0 * np.square(cs)
+
+
+def elastic_chi(medium: ElasticMedium):
+    """solver/elastic.jl:177-195: Kelvin-Voigt factors chi = 2 db2neper(alpha, y) c_ref^(y-1),
+    c_ref the (mean) compressional or shear speed; 0 when the coefficient or alpha_power is unset."""
+    y = medium.alpha_power
+    chi_p = chi_s = 0.0
+    if medium.alpha_coeff_compression is not None and y is not None:
+        cp = medium.sound_speed_compression
+        c_ref = float(cp) if _is_scalar(cp) else float(np.mean(cp))
+        chi_p = 2 * db2neper(medium.alpha_coeff_compression, y) * c_ref ** (y - 1)
+    if medium.alpha_coeff_shear is not None and y is not None:
+        cs = medium.sound_speed_shear
+        cs_ref = float(cs) if _is_scalar(cs) else float(np.mean(cs))
+        chi_s = 2 * db2neper(medium.alpha_coeff_shear, y) * cs_ref ** (y - 1)
+    return chi_p, chi_s
+
+
+def pstd_elastic(grid: KWaveGrid, medium: ElasticMedium, source: ElasticSource, sensor: KWaveSensor,
+                 pml_size=None, pml_alpha=2.0, dtype=np.float64, max_steps: Optional[int] = None,
+                 progress_callback=None) -> dict:
+    """Restates ``pstd_elastic_2d`` (solver/elastic.jl:133-366) and ``pstd_elastic_3d``
+    (:386-588): the stress-velocity PSTD scheme on a staggered grid.
+
+    Per step: the stress divergence (sum over d of d/dx_d sigma_{dj}, staggered +) updates each
+    velocity with its own split PML and 1/rho_sg (:236-250, 471-481); velocity sources (:253-276);
+    the nine (four in 2D) velocity gradients (staggered -) update the stresses (:279-313, 505-521)
+    -- the Kelvin-Voigt factors chi_p, chi_s enter only the 2D homogeneous branch -- then stress
+    sources (:316-347), and the sensor records p = -trace(sigma)/D with the velocities (:350-356,
+    565-570).  p0 sets every normal stress to -p0 (no smoothing).  Default pml_size is 20 in 2D and
+    10 in 3D, as in the reference signatures.  ``max_steps`` (oracle only) stops early.
+    """
+    if grid.Nt == 0 or grid.dt == 0:
+        raise RuntimeError("Time array not set. Call make_time!(kgrid, sound_speed) before running.")
+    for f in sensor.record:
+        if f not in VALID_RECORD_FIELDS:
+            raise ValueError(f"Invalid sensor record field: :{f}")
+    D = grid.ndim
+    if D not in (2, 3):
+        raise TypeError("pstd_elastic_2d / pstd_elastic_3d take a 2D or 3D grid")
+    if pml_size is None:
+        pml_size = 20 if D == 2 else 10
+    shape, dt, Nt = grid.N, grid.dt, grid.Nt
+    ct = np.complex64 if dtype == np.float32 else np.complex128
+    psz = tuple(pml_size) if isinstance(pml_size, (tuple, list)) else (pml_size,) * D
+    pal = tuple(pml_alpha) if isinstance(pml_alpha, (tuple, list)) else (pml_alpha,) * D
+
+    def bshape(v, d):
+        s = [1] * D
+        s[d] = -1
+        return v.reshape(s)
+
+    pml = [bshape(get_pml(shape[d], grid.d[d], psz[d], pal[d], dt), d) for d in range(D)]
+    pml_sg = [bshape(get_pml(shape[d], grid.d[d], psz[d], pal[d], dt, staggered=True), d) for d in range(D)]
+
+    lam, mu = elastic_lame(medium)
+    homogeneous = _is_scalar(lam)
+    chi_p, chi_s = elastic_chi(medium) if D == 2 else (0.0, 0.0)
+    rho0 = medium.density if _is_scalar(medium.density) else np.asarray(medium.density, np.float64)
+    rho_sg = None if _is_scalar(rho0) else [stagger_density(rho0, d) for d in range(D)]
+
+    plans = _Plans(shape)
+    k_ops = [grid.k_vecs[d].astype(dtype) for d in range(D)]
+    s_pos = [grid.shift_pos[d].astype(ct) for d in range(D)]
+    s_neg = [grid.shift_neg[d].astype(ct) for d in range(D)]
+
+    zeros = lambda: np.zeros(shape, dtype=np.float64, order="F")
+    v = [zeros() for _ in range(D)]
+    slots = [0, 1, 3] if D == 2 else list(range(6))
+    sig = {k: zeros() for k in slots}
+
+    sensor_data = _create_sensor_data(sensor, Nt)
+    mask_idx = findall(sensor.mask) if (sensor.mask is not None and np.asarray(sensor.mask).dtype == bool) \
+        else np.zeros(0, dtype=np.int64)
+
+    if source.p0 is not None:
+        p0 = np.asarray(source.p0, dtype=np.float64)
+        for d in range(D):
+            sig[d][...] = -p0
+
+    u_idx = findall(source.u_mask) if source.u_mask is not None else None
+    s_idx = findall(source.s_mask) if source.s_mask is not None else None
+    u_sigs = [None if s is None else _signal_2d(s) for s in (source.ux, source.uy, source.uz)][:D]
+    s_sigs = [None if s is None else _signal_2d(s) for s in
+              (source.sxx, source.syy, source.szz, source.sxy, source.sxz, source.syz)]
+
+    def inject(fields, sigs, idx, mode, t_index):
+        for f, sg in zip(fields, sigs):
+            if sg is None:
+                continue
+            col = sg[:, 0] if sg.shape[1] == 1 else sg[:, min(t_index, sg.shape[1]) - 1]
+            vals = col[: len(idx)]
+            ff = _flatF(f)
+            if mode == DIRICHLET:
+                ff[idx] = vals
+            else:
+                ff[idx] = ff[idx] + vals
+
+    grad = lambda f, d, sp: spectral_gradient(f, k_ops[d], sp[d], plans, d, dtype).astype(np.float64)
+    steps = Nt if max_steps is None else min(Nt, max_steps)
+    p = zeros()
+    for t_index in range(1, steps + 1):
+        # stress divergence -> velocities (x, y[, z] terms summed in that order)
+        for j in range(D):
+            acc = grad(sig[stress_slot(0, j)], 0, s_pos)
+            for d in range(1, D):
+                acc = acc + grad(sig[stress_slot(d, j)], d, s_pos)
+            rs = rho0 if rho_sg is None else rho_sg[j]
+            v[j][...] = pml_sg[j] * (pml_sg[j] * v[j] + dt / rs * acc)
+        if u_idx is not None:
+            inject(v, u_sigs, u_idx, source.u_mode, t_index)
+        # velocity gradients dv_j/dx_d
+        g = [[grad(v[j], d, s_neg) for d in range(D)] for j in range(D)]  # g[j][d]
+        l2m = lam + 2 * mu
+        if D == 2:
+            dxx, dyy = g[0][0], g[1][1]
+            a_xx = l2m * dxx + lam * dyy
+            a_yy = lam * dxx + l2m * dyy
+            sh = mu * (g[0][1] + g[1][0])
+            if homogeneous:
+                a_xx = a_xx + chi_p * (l2m * dxx + lam * dyy)
+                a_yy = a_yy + chi_p * (lam * dxx + l2m * dyy)
+                sh = sh + chi_s * mu * (g[0][1] + g[1][0])
+            sig[0][...] = pml[0] * (pml[0] * sig[0] + dt * a_xx)
+            sig[1][...] = pml[1] * (pml[1] * sig[1] + dt * a_yy)
+            sig[3][...] = pml[0] * pml[1] * (sig[3] + dt * sh)
+        else:
+            dxx, dyy, dzz = g[0][0], g[1][1], g[2][2]
+            sig[0][...] = pml[0] * (pml[0] * sig[0] + dt * (l2m * dxx + lam * (dyy + dzz)))
+            sig[1][...] = pml[1] * (pml[1] * sig[1] + dt * (l2m * dyy + lam * (dxx + dzz)))
+            sig[2][...] = pml[2] * (pml[2] * sig[2] + dt * (l2m * dzz + lam * (dxx + dyy)))
+            sig[3][...] = pml[0] * pml[1] * (sig[3] + dt * mu * (g[0][1] + g[1][0]))
+            sig[4][...] = pml[0] * pml[2] * (sig[4] + dt * mu * (g[0][2] + g[2][0]))
+            sig[5][...] = pml[1] * pml[2] * (sig[5] + dt * mu * (g[1][2] + g[2][1]))
+        if s_idx is not None:
+            inject([sig[k] for k in slots], [s_sigs[k] for k in slots], s_idx, source.s_mode, t_index)
+        p[...] = -(sum(sig[d] for d in range(D))) / D
+        if len(mask_idx) > 0:
+            _record(sensor_data, sensor.record, p, v, mask_idx, t_index, Nt)
+        if progress_callback is not None:
+            progress_callback(t_index, Nt, p)
+
+    if "p_rms" in sensor_data:
+        sensor_data["p_rms"] = np.sqrt(sensor_data["p_rms"] / Nt)
+    if "u_rms" in sensor_data:
+        sensor_data["u_rms"] = np.sqrt(sensor_data["u_rms"] / Nt)
+    return sensor_data
+
+
+def pstd_elastic_2d(grid, medium, source, sensor, pml_size=20, pml_alpha=2.0, **kw) -> dict:
+    """solver/elastic.jl:133-366."""
+    if grid.ndim != 2:
+        raise TypeError("pstd_elastic_2d takes a KWaveGrid2D")
+    return pstd_elastic(grid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha, **kw)
+
+
+def pstd_elastic_3d(grid, medium, source, sensor, pml_size=10, pml_alpha=2.0, **kw) -> dict:
+    """solver/elastic.jl:386-588."""
+    if grid.ndim != 3:
+        raise TypeError("pstd_elastic_3d takes a KWaveGrid3D")
+    return pstd_elastic(grid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha, **kw)

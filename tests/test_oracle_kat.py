@@ -320,3 +320,133 @@ def test_axisymmetric_radial_term():
     b = K.kspace_first_order(g, med, K.KWaveSource(p0=p0), K.KWaveSensor(mask=mask, record=["p_final"]), pml_size=4)
     rel = np.linalg.norm(a["p_final"] - b["p_final"]) / np.linalg.norm(b["p_final"])
     assert rel > 1e-3
+
+
+# ---- test_elastic.jl, and closed-form plane waves of the elastic scheme ----------------------
+
+def _elastic_medium():
+    return K.ElasticMedium(sound_speed_compression=3000.0, sound_speed_shear=1500.0, density=1800.0)
+
+
+def test_elastic_medium_and_source_construction():  # test_elastic.jl:2-42
+    em = _elastic_medium()
+    assert em.alpha_coeff_compression is None and em.alpha_coeff_shear is None
+    em2 = K.ElasticMedium(3000.0, 1500.0, 1800.0, alpha_coeff_compression=0.5, alpha_coeff_shear=1.0,
+                          alpha_power=1.5)
+    chi_p, chi_s = K.elastic_chi(em2)
+    assert chi_p == pytest.approx(2 * K.db2neper(0.5, 1.5) * 3000.0 ** 0.5, rel=1e-15)
+    assert chi_s == pytest.approx(2 * K.db2neper(1.0, 1.5) * 1500.0 ** 0.5, rel=1e-15)
+    es = K.ElasticSource()
+    assert es.s_mask is None and es.p0 is None and es.s_mode == K.ADDITIVE
+    lam, mu = K.elastic_lame(em)
+    assert lam == 1800.0 * (3000.0 ** 2 - 2 * 1500.0 ** 2) and mu == 1800.0 * 1500.0 ** 2
+    with pytest.raises(TypeError):  # the reference evaluates cp^2 as a matrix power here
+        K.elastic_lame(K.ElasticMedium(np.full((4, 4), 3000.0), 1500.0, 1800.0))
+
+
+def test_elastic_2d_basic_runs():  # test_elastic.jl:44-124
+    for n, src in ((32, "p0"), (32, "stress"), (64, "p0")):
+        g = K.KWaveGrid(n, 0.5e-3, n, 0.5e-3)
+        K.make_time(g, 3000.0)
+        mask = np.zeros((n, n), bool)
+        if src == "p0":
+            p0 = np.zeros((n, n))
+            p0[n // 2 - 1, n // 2 - 1] = 1.0
+            source = K.ElasticSource(p0=p0)
+            if n == 64:
+                mask[n // 4 - 1, n // 2 - 1] = True
+            else:
+                mask[4, :] = True
+        else:
+            s_mask = np.zeros((n, n), bool)
+            s_mask[4, n // 2 - 1] = True
+            sig = np.sin(2 * math.pi * 1e6 * np.arange(g.Nt) * g.dt).reshape(1, -1)
+            source = K.ElasticSource(s_mask=s_mask, sxx=sig, s_mode=K.ADDITIVE)
+            mask[n // 2 - 1, :] = True
+        r = K.pstd_elastic_2d(g, _elastic_medium(), source, K.KWaveSensor(mask=mask, record=["p"]))
+        assert r["p"].shape == (mask.sum(), g.Nt)
+        assert np.all(np.isfinite(r["p"])) and np.abs(r["p"]).max() > 0
+
+
+def test_elastic_3d_basic_run():  # test_elastic.jl:126-153
+    n = 16
+    g = K.KWaveGrid(n, 0.5e-3, n, 0.5e-3, n, 0.5e-3)
+    K.make_time(g, 3000.0)
+    p0 = np.zeros((n, n, n))
+    p0[n // 2 - 1, n // 2 - 1, n // 2 - 1] = 1.0
+    mask = np.zeros((n, n, n), bool)
+    mask[2, :, :] = True
+    r = K.pstd_elastic_3d(g, _elastic_medium(), K.ElasticSource(p0=p0), K.KWaveSensor(mask=mask, record=["p"]),
+                          pml_size=5)
+    assert r["p"].shape == (mask.sum(), g.Nt) and np.all(np.isfinite(r["p"]))
+
+
+def _plane_wave_modes(n, dx, m):
+    """Full-FFT wavenumbers of an x line and the staggered gradient multipliers i k e^{+-ik dx/2}."""
+    g = K.KWaveGrid(n, dx)
+    k = g.k_vecs[0]
+    return k, 1j * k * np.exp(1j * k * dx / 2), 1j * k * np.exp(-1j * k * dx / 2)
+
+
+@pytest.mark.parametrize("D", [2, 3])
+def test_elastic_p_wave_matches_leapfrog_recurrence(D):
+    """A plane compressional wave along x in a homogeneous medium without PML: per Fourier mode,
+    v <- v + dt/rho G+ s_xx; s_xx <- s_xx + dt (lambda + 2 mu) G- v; s_yy (, s_zz) <- ... + dt lambda G- v."""
+    n, dx, steps = 32, 0.5e-3, 60
+    args = []
+    for _ in range(D):
+        args += [n, dx]
+    g = K.KWaveGrid(*args)
+    g.dt, g.Nt = 5e-8, steps
+    x = np.arange(n)
+    line = np.cos(2 * math.pi * 3 * x / n) + 0.5 * np.sin(2 * math.pi * 5 * x / n)
+    p0 = np.broadcast_to(line.reshape((-1,) + (1,) * (D - 1)), g.N).copy()
+    mask = np.zeros(g.N, bool)
+    mask[(slice(None),) + (1,) * (D - 1)] = True
+    rho, cp, cs = 1800.0, 3000.0, 1500.0
+    r = K.pstd_elastic(g, K.ElasticMedium(cp, cs, rho), K.ElasticSource(p0=p0),
+                       K.KWaveSensor(mask=mask, record=["p", "ux"]), pml_size=0)
+    lam, mu = rho * (cp ** 2 - 2 * cs ** 2), rho * cs ** 2
+    _, gp, gn = _plane_wave_modes(n, dx, 0)
+    S = -np.fft.fft(line)
+    T = S.copy()
+    V = np.zeros(n, complex)
+    p_ref, u_ref = np.zeros((n, steps)), np.zeros((n, steps))
+    for t in range(steps):
+        V = V + g.dt / rho * gp * S
+        S, T = S + g.dt * (lam + 2 * mu) * gn * V, T + g.dt * lam * gn * V
+        p_ref[:, t] = np.real(np.fft.ifft(-(S + (D - 1) * T) / D))
+        u_ref[:, t] = np.real(np.fft.ifft(V))
+    assert np.allclose(r["p"], p_ref, rtol=0, atol=1e-12 * np.abs(p_ref).max())
+    assert np.allclose(r["ux"], u_ref, rtol=0, atol=1e-12 * np.abs(u_ref).max())
+
+
+def test_elastic_s_wave_matches_leapfrog_recurrence():
+    """A transverse velocity kick vy = f(x) at step 1 (additive source over the whole grid): a plane
+    shear wave, per mode vy <- vy + dt/rho G+ s_xy, s_xy <- s_xy + dt mu G- vy; p stays 0."""
+    n, dx, steps = 32, 0.5e-3, 50
+    g = K.KWaveGrid(n, dx, n, dx)
+    g.dt, g.Nt = 5e-8, steps
+    x = np.arange(n)
+    line = np.cos(2 * math.pi * 2 * x / n)
+    u_mask = np.ones((n, n), bool)
+    kick = np.zeros((n * n, steps))
+    kick[:, 0] = np.tile(line, n)  # column-major points: x fastest
+    mask = np.zeros((n, n), bool)
+    mask[:, 3] = True
+    rho, cp, cs = 1800.0, 3000.0, 1500.0
+    r = K.pstd_elastic_2d(g, K.ElasticMedium(cp, cs, rho), K.ElasticSource(u_mask=u_mask, uy=kick),
+                          K.KWaveSensor(mask=mask, record=["p", "uy"]), pml_size=0)
+    mu = rho * cs ** 2
+    _, gp, gn = _plane_wave_modes(n, dx, 0)
+    V = np.zeros(n, complex)
+    Sxy = np.zeros(n, complex)
+    u_ref = np.zeros((n, steps))
+    for t in range(steps):
+        V = V + g.dt / rho * gp * Sxy
+        if t == 0:
+            V = V + np.fft.fft(line)
+        Sxy = Sxy + g.dt * mu * gn * V
+        u_ref[:, t] = np.real(np.fft.ifft(V))
+    assert np.allclose(r["uy"], u_ref, rtol=0, atol=1e-12)
+    assert np.abs(r["p"]).max() < 1e-12
