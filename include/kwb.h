@@ -130,6 +130,21 @@ typedef struct kwb_problem {
    * x axial, y radial; the radial density update adds u_r / r to the divergence, r = |y_vec|
    * with r = 0 replaced by dy/2.  Time-reversal data is not accepted with it. */
   int32_t axisymmetric;
+
+  /* 1: the elastic stress-velocity solver, pstd_elastic_2d / pstd_elastic_3d
+   * (solver/elastic.jl:133-366, 386-588); ndim 2 or 3.  c0 holds sound_speed_compression, cs
+   * sound_speed_shear and rho0 the density (an array density when either speed is an array:
+   * with a scalar density the reference squares an array speed as a matrix, elastic.jl:169).
+   * alpha_mode != KWB_NO_ABSORPTION carries alpha_coeff_compression in alpha_coeff (with
+   * alpha_power); has_alpha_shear / alpha_coeff_shear the shear coefficient.  p0 sets every normal
+   * stress to -p0 (not smoothed); the velocity source is u_*; s_* are the stress sources.  BonA,
+   * pressure sources, time reversal and the axisymmetric flag are not part of it. */
+  int32_t elastic;
+  kwb_field cs;
+  int32_t has_alpha_shear;
+  double alpha_coeff_shear;
+  const int64_t *s_index; int64_t n_s_index; int32_t s_mode;
+  kwb_signal s_signal[6]; /* sxx, syy, szz, sxy, sxz, syz (2D: sxx, syy, sxy; szz/sxz/syz unused) */
 } kwb_problem;
 
 /* Output sizes of one group: rows x cols per field, 0 x 0 when the field is not recorded. */

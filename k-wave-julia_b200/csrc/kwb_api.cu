@@ -309,6 +309,31 @@ int validate_problem(kwb_ctx *ctx, const kwb_problem *P) {
     return KWB_OK;
   };
   int rc;
+  if (P->elastic) {
+    if (P->ndim < 2) return set_err(ctx, KWB_E_INVALID, "the elastic solver takes a 2D or 3D grid");
+    if (P->axisymmetric || P->tr.data)
+      return set_err(ctx, KWB_E_INVALID, "time reversal and the axisymmetric form are not part of the elastic solver");
+    if (P->BonA.count) return set_err(ctx, KWB_E_INVALID, "B/A is not part of the elastic solver");
+    if (P->n_p_index > 0)
+      return set_err(ctx, KWB_E_INVALID, "the elastic solver has stress sources, not pressure sources");
+    if ((rc = chk_field(P->cs, "sound_speed_shear", false))) return rc;
+    const bool speed_arr = (P->c0.count == nvox || P->cs.count == nvox) && nvox > 1;
+    if (speed_arr && !(P->rho0.count == nvox && nvox > 1))
+      return set_err(ctx, KWB_E_INVALID,
+                     "a scalar density with array wave speeds is evaluated as a matrix power (cp^2) by the "
+                     "reference (solver/elastic.jl:169); give the density as an array");
+    if (P->has_alpha_shear && !(std::isfinite(P->alpha_coeff_shear) && std::isfinite(P->alpha_power)))
+      return set_err(ctx, KWB_E_INVALID, "alpha_coeff_shear and alpha_power must be set for shear absorption");
+    if ((rc = validate_index(ctx, P->s_index, P->n_s_index, nvox, "s_mask"))) return rc;
+    for (int k = 0; k < 6; ++k) {
+      if (!P->s_signal[k].data || P->n_s_index == 0) continue;
+      if (P->s_signal[k].n_rows < P->n_s_index || P->s_signal[k].n_cols < 1)
+        return set_err(ctx, KWB_E_INVALID, "BoundsError: stress source %d has %lld rows for %lld s_mask points",
+                       k, (long long)P->s_signal[k].n_rows, (long long)P->n_s_index);
+    }
+  } else if (P->n_s_index > 0) {
+    return set_err(ctx, KWB_E_INVALID, "stress sources belong to the elastic solver");
+  }
   if ((rc = chk_field(P->c0, "sound_speed", false))) return rc;
   if ((rc = chk_field(P->rho0, "density", true))) return rc;
   if ((rc = chk_field(P->BonA, "BonA", true))) return rc;
@@ -416,11 +441,69 @@ int fill_f64(kwb_ctx *ctx, double *p, long long n, double v, cudaStream_t st) {
   return KWB_OK;
 }
 
+// One elastic time step (kwb_elastic.cu).  run(name, algorithmic bytes, launcher) issues each
+// launch, so the same sequence serves the captured step and the per-kernel profile.
+template <class Run>
+cudaError_t elastic_step(kwb_sim *S, long long s, Run &&run) {
+  const SimDev &h = S->h;
+  cudaStream_t st = S->stream;
+  const int D = h.ndim;
+  const double nv = (double)h.nvox;
+  static const char *gname[2][3] = {{"el_grad_stress_x", "el_grad_stress_y", "el_grad_stress_z"},
+                                    {"el_grad_velocity_x", "el_grad_velocity_y", "el_grad_velocity_z"}};
+  cudaError_t e;
+  // stress divergence: the pass along d adds d/dx_d sigma_dj to w_j
+  for (int d = 0; d < D; ++d) {
+    ElGrad g{};
+    g.nf = D;
+    for (int j = 0; j < D; ++j) {
+      g.src[j] = h.el_s[kwb_stress_slot(d, j)];
+      g.dst[j] = h.el_w[j];
+    }
+    g.acc = d > 0 ? 7 : 0;
+    g.neg = 0;
+    if ((e = run(gname[0][d], nv * 4.0 * D * (d > 0 ? 3 : 2), [&] { return el_grad(h, d, g, s, st); })) != cudaSuccess)
+      return e;
+  }
+  if ((e = run("el_velocity", nv * 4.0 * (3 * D + (h.rho0 ? 2 : 0)), [&] { return el_velocity(h, s, st); })) != cudaSuccess)
+    return e;
+  if (h.n_u > 0 && (e = run("el_inject", 0.0, [&] { return el_inject(h, 0, s, st); })) != cudaSuccess) return e;
+  // velocity gradients: dv_d/dx_d into w_d, dv_j/dx_d into the shear slot {d, j} (first writer
+  // is the pass along the smaller axis, the other adds)
+  for (int d = 0; d < D; ++d) {
+    ElGrad g{};
+    g.nf = D;
+    int reads = D;
+    for (int j = 0; j < D; ++j) {
+      g.src[j] = h.u[j];
+      g.dst[j] = h.el_w[kwb_stress_slot(d, j)];
+      if (j < d) {
+        g.acc |= 1 << j;
+        ++reads;
+      }
+    }
+    g.neg = 1;
+    if ((e = run(gname[1][d], nv * 4.0 * (reads + D), [&] { return el_grad(h, d, g, s, st); })) != cudaSuccess)
+      return e;
+  }
+  const int ns = D == 2 ? 3 : 6;
+  if ((e = run("el_stress", nv * 4.0 * (3 * ns + 1 + (h.el_lam ? 2 : 0)), [&] { return el_stress(h, s, st); })) != cudaSuccess)
+    return e;
+  if (h.n_s > 0 && (e = run("el_inject", 0.0, [&] { return el_inject(h, 1, s, st); })) != cudaSuccess) return e;
+  for (auto &g : S->groups) {
+    if (g.spec.cartesian || g.n == 0) continue;
+    if ((e = run("sensor_gather", 0.0, [&] { return launch_sensor_gather(S->d_sim, h, g.d_dev, g.n, s, st); })) != cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
+}
+
 // Enqueue one time step (eager).  step_s is relative to the device step base.
 cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
   const SimDev &h = S->h;
   cudaStream_t st = S->stream;
   cudaError_t e;
+  if (h.elastic) return elastic_step(S, step_s, [](const char *, double, auto fn) { return fn(); });
   if (S->tr && (e = launch_tr_inject(S->d_sim, h, step_s, st)) != cudaSuccess) return e;
   // line passes: y, z, then x
   for (int a : {1, 2, 0}) {
@@ -446,6 +529,12 @@ cudaError_t enqueue_step(kwb_sim *S, long long step_s) {
 }
 
 int count_launches(const kwb_sim *S) {
+  if (S->h.elastic) {
+    int n = 2 * S->h.ndim + 2 + (S->h.n_u > 0 ? 1 : 0) + (S->h.n_s > 0 ? 1 : 0);
+    for (auto &g : S->groups)
+      if (!g.spec.cartesian && g.n > 0) ++n;
+    return n;
+  }
   int n = (S->tr ? 1 : 0) + S->h.ndim + (S->h.fuse_xeos ? 1 : 2) + (S->h.ndim == 2 ? 1 : (S->h.ndim == 3 ? (S->h.plane ? 1 : 3) : 0));
   for (auto &g : S->groups)
     if (!g.spec.cartesian && g.n > 0 && !g.fused) ++n;
@@ -466,14 +555,26 @@ size_t estimate_device_bytes(const kwb_problem *P) {
   const bool r_arr = P->rho0.count == nvox && nvox > 1;
   const bool b_arr = P->BonA.count == nvox && nvox > 1;
   const bool nonlinear = P->BonA.count > 0;
-  const bool dispersion = !c_arr && P->alpha_mode == KWB_STOKES;
-  size_t need = (size_t)nvox * 4 * (1 + 2 * D) + (size_t)nspec * 8;
-  if (dispersion) need += (size_t)nvox * 4 + (size_t)nspec * 8;
-  need += (size_t)nspec * 4 * (dispersion ? 2 : 1);
-  need += (size_t)nvox * 4 * ((r_arr ? 1 : 0) + (c_arr ? 1 : 0) + ((nonlinear && (b_arr || r_arr)) ? 1 : 0));
-  // FP64 staging during set-up (released once the simulation is created)
-  if (c_arr || r_arr || b_arr || P->p0.count)
-    need += (size_t)nvox * 8 * (((nonlinear && b_arr && r_arr) ? 2 : 1) + ((P->row_major && D > 1) ? 1 : 0));
+  const bool dispersion = !c_arr && P->alpha_mode == KWB_STOKES && !P->elastic;
+  size_t need;
+  if (P->elastic) {
+    // p, velocities, stresses and derivative scratch; rho0, lambda and mu per voxel with an array
+    // density; FP64 staging of one array during set-up
+    const int ns = D == 2 ? 3 : 6;
+    need = (size_t)nvox * 4 * (1 + D + 2 * ns) + (size_t)nvox * 4 * (r_arr ? 3 : 0);
+    if (r_arr || P->p0.count) need += (size_t)nvox * 8 * (1 + ((P->row_major && D > 1) ? 1 : 0));
+    for (int k = 0; k < 6; ++k)
+      if (P->s_signal[k].data) need += (size_t)P->s_signal[k].n_rows * P->s_signal[k].n_cols * 12;
+    need += (size_t)P->n_s_index * 8 + (size_t)P->n_u_index * 8;
+  } else {
+    need = (size_t)nvox * 4 * (1 + 2 * D) + (size_t)nspec * 8;
+    if (dispersion) need += (size_t)nvox * 4 + (size_t)nspec * 8;
+    need += (size_t)nspec * 4 * (dispersion ? 2 : 1);
+    need += (size_t)nvox * 4 * ((r_arr ? 1 : 0) + (c_arr ? 1 : 0) + ((nonlinear && (b_arr || r_arr)) ? 1 : 0));
+    // FP64 staging during set-up (released once the simulation is created)
+    if (c_arr || r_arr || b_arr || P->p0.count)
+      need += (size_t)nvox * 8 * (((nonlinear && b_arr && r_arr) ? 2 : 1) + ((P->row_major && D > 1) ? 1 : 0));
+  }
   for (int g = 0; g < P->n_groups; ++g) {
     const kwb_sensor_group &G = P->groups[g];
     if (G.cartesian) continue;
@@ -609,6 +710,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   S->Nt_grid = P->Nt;
   S->Nt_loop = S->tr ? P->tr.n_cols : P->Nt;
   h.Nt = S->Nt_loop;
+  h.elastic = P->elastic ? 1 : 0;
 
   // ---- medium scalars / flags
   const bool c_arr = P->c0.count == nvox && nvox > 1;
@@ -623,7 +725,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   const bool nonlinear = P->BonA.count > 0;
   h.nonlinear = nonlinear;
   h.scalar_c = !c_arr;
-  h.dispersion = (!c_arr && absorbing && P->alpha_mode == KWB_STOKES) ? 1 : 0;
+  h.dispersion = (!c_arr && absorbing && P->alpha_mode == KWB_STOKES && !h.elastic) ? 1 : 0;
   h.dt_over_rho0_s = (float)(P->dt / r_s);
   h.dt_rho0_s = (float)(P->dt * r_s);
   h.c0sq_s = (float)(c_s * c_s);
@@ -648,6 +750,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (tv && strcmp(tv, "big") == 0) h.tile_override = 0;
     if (tv && strcmp(tv, "mid") == 0) h.tile_override = 1;
     if (tv && strcmp(tv, "small") == 0) h.tile_override = 2;
+    if (h.elastic) h.fast = 0;  // the elastic passes run on the generic line FFTs
   }
 
   // ---- tile shapes and FFT plans
@@ -677,11 +780,21 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   CU(cudaMemsetAsync(h.p, 0, nvox * 4, st));
   for (int d = 0; d < D; ++d) {
     CU(M.alloc(&h.u[d], nvox));
-    CU(M.alloc(&h.rho[d], nvox));
     CU(cudaMemsetAsync(h.u[d], 0, nvox * 4, st));
+    if (h.elastic) continue;
+    CU(M.alloc(&h.rho[d], nvox));
     CU(cudaMemsetAsync(h.rho[d], 0, nvox * 4, st));
   }
-  CU(M.alloc(&h.spec, h.nspec));
+  if (h.elastic) {
+    for (int k = 0; k < 6; ++k) {
+      if (D == 2 && (k == 2 || k > 3)) continue;  // 2-D: xx, yy, xy
+      CU(M.alloc(&h.el_s[k], nvox));
+      CU(M.alloc(&h.el_w[k], nvox));
+      CU(cudaMemsetAsync(h.el_s[k], 0, nvox * 4, st));
+    }
+  } else {
+    CU(M.alloc(&h.spec, h.nspec));
+  }
   if (h.dispersion) {
     CU(M.alloc(&h.spec2, h.nspec));
     CU(M.alloc(&h.rho_prev, nvox));
@@ -706,43 +819,89 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     CU(transpose_to_column_major(dst, rm_in, D, h.N, st));
     return KWB_OK;
   };
-  if (c_arr) {
-    float *c0sq;
-    CU(M.alloc(&c0sq, nvox));
-    if ((rc = upload_grid(stage, P->c0.data))) return rc;
-    CU(convert_f64_to_f32(c0sq, stage, nvox, 1, st));
-    h.c0sq = c0sq;
-  }
-  // rho0 stays staged in FP64 for the nonlinearity term (stage2 when B/A is an array too)
-  double *rho_stage = stage2 ? stage2 : stage;
-  if (r_arr) {
-    float *rho0;
-    CU(M.alloc(&rho0, nvox));
-    if ((rc = upload_grid(rho_stage, P->rho0.data))) return rc;
-    CU(convert_f64_to_f32(rho0, rho_stage, nvox, 0, st));
-    h.rho0 = rho0;
-  }
-  if (nonlinear) {
-    const double b_s = P->BonA.data[0];
-    if (b_arr || r_arr) {
-      float *q;
-      CU(M.alloc(&q, nvox));
-      const double *bp = nullptr, *rp = nullptr;
-      if (b_arr && r_arr) {
-        if ((rc = upload_grid(stage, P->BonA.data))) return rc;
-        bp = stage;
-        rp = stage2;
-      } else if (b_arr) {
-        if ((rc = upload_grid(stage, P->BonA.data))) return rc;
-        bp = stage;
-      } else {
-        rp = stage;
-      }
-      CU(build_nlq(q, bp, b_arr, b_s, rp, r_arr, r_s, nvox, st));
-      h.nlq = q;
+  if (h.elastic) {
+    // lambda = rho0 (cp^2 - 2 cs^2), mu = rho0 cs^2 in FP64 (solver/elastic.jl:168-174, 419-423),
+    // per voxel in the input's memory order when the density is an array (the speeds then may
+    // be arrays or scalars), else scalars
+    const bool cs_arr = P->cs.count == nvox && nvox > 1;
+    const double cs_s = P->cs.data[0];
+    if (r_arr) {
+      std::vector<double> lam(nvox), mu(nvox);
+      parallel_range(nvox, [&](long long lo, long long hi) {
+        for (long long i = lo; i < hi; ++i) {
+          const double cp = c_arr ? P->c0.data[i] : c_s, cs = cs_arr ? P->cs.data[i] : cs_s;
+          const double rho = P->rho0.data[i];
+          lam[i] = rho * (cp * cp - 2.0 * cs * cs);
+          mu[i] = rho * (cs * cs);
+        }
+      });
+      float *dl, *dm, *rho0;
+      CU(M.alloc(&dl, nvox));
+      CU(M.alloc(&dm, nvox));
+      CU(M.alloc(&rho0, nvox));
+      if ((rc = upload_grid(stage, lam.data()))) return rc;
+      CU(convert_f64_to_f32(dl, stage, nvox, 0, st));
+      if ((rc = upload_grid(stage, mu.data()))) return rc;
+      CU(convert_f64_to_f32(dm, stage, nvox, 0, st));
+      if ((rc = upload_grid(stage, P->rho0.data))) return rc;
+      CU(convert_f64_to_f32(rho0, stage, nvox, 0, st));
+      CU(cudaStreamSynchronize(st));  // the host arrays go out of scope
+      h.el_lam = dl;
+      h.el_mu = dm;
+      h.rho0 = rho0;
     } else {
-      h.nlq_s = (float)((b_s / 2.0) / r_s);
+      h.el_lam_s = (float)(r_s * (c_s * c_s - 2.0 * cs_s * cs_s));
+      h.el_mu_s = (float)(r_s * (cs_s * cs_s));
+      // Kelvin-Voigt factors chi = 2 db2neper(alpha, y) c^(y-1), used by the 2-D homogeneous
+      // branch only (elastic.jl:177-195, 282-295)
+      auto chi = [&](double alpha, double c) {
+        const double y = P->alpha_power;
+        const double a_np = alpha * (1e-2 / (20.0 * std::log10(std::exp(1.0)))) * std::pow(2.0 * kPi * 1e6, -y);
+        return 2.0 * a_np * std::pow(c, y - 1.0);
+      };
+      if (D == 2 && absorbing) h.el_chi_p = (float)chi(P->alpha_coeff, c_s);
+      if (D == 2 && P->has_alpha_shear) h.el_chi_s = (float)chi(P->alpha_coeff_shear, cs_s);
     }
+  } else {
+    if (c_arr) {
+      float *c0sq;
+      CU(M.alloc(&c0sq, nvox));
+      if ((rc = upload_grid(stage, P->c0.data))) return rc;
+      CU(convert_f64_to_f32(c0sq, stage, nvox, 1, st));
+      h.c0sq = c0sq;
+    }
+    // rho0 stays staged in FP64 for the nonlinearity term (stage2 when B/A is an array too)
+    double *rho_stage = stage2 ? stage2 : stage;
+    if (r_arr) {
+      float *rho0;
+      CU(M.alloc(&rho0, nvox));
+      if ((rc = upload_grid(rho_stage, P->rho0.data))) return rc;
+      CU(convert_f64_to_f32(rho0, rho_stage, nvox, 0, st));
+      h.rho0 = rho0;
+    }
+    if (nonlinear) {
+      const double b_s = P->BonA.data[0];
+      if (b_arr || r_arr) {
+        float *q;
+        CU(M.alloc(&q, nvox));
+        const double *bp = nullptr, *rp = nullptr;
+        if (b_arr && r_arr) {
+          if ((rc = upload_grid(stage, P->BonA.data))) return rc;
+          bp = stage;
+          rp = stage2;
+        } else if (b_arr) {
+          if ((rc = upload_grid(stage, P->BonA.data))) return rc;
+          bp = stage;
+        } else {
+          rp = stage;
+        }
+        CU(build_nlq(q, bp, b_arr, b_s, rp, r_arr, r_s, nvox, st));
+        h.nlq = q;
+      } else {
+        h.nlq_s = (float)((b_s / 2.0) / r_s);
+      }
+    }
+
   }
 
   // ---- per-axis tables (FP64 on device)
@@ -792,7 +951,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     const char *fx = getenv("KWB_FUSE_XEOS");
     h.fuse_xeos = (h.fast & 3) == 3 && D >= 2 && !h.dispersion && fast_size(h.N[0]) && !(fx && strcmp(fx, "0") == 0);
   }
-  {
+  if (!h.elastic) {
     float *Mt, *M2 = nullptr;
     CU(M.alloc(&Mt, h.nspec));
     if (h.dispersion) CU(M.alloc(&M2, h.nspec));
@@ -875,6 +1034,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
       CU(M.alloc(&tab, n * sg.n_cols));
       CU(build_source_table(tab, sig, sg.n_rows, n, sg.n_cols, nullptr, 1.0, 0, 1.0, 0, st));
       h.u_sig[a] = tab;
+      if (h.elastic) continue;  // injected at point lists (below), not inside line passes
       std::vector<int> ptr;
       std::vector<SrcEntry> ent;
       build_csr(P->u_index, n, h.N, a, ptr, ent);
@@ -888,6 +1048,35 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
       h.u_line_ptr[a] = dptr;
       h.u_entry[a] = dent;
     }
+  }
+
+  if (h.elastic && P->n_u_index > 0) {
+    long long *di;
+    CU(M.alloc(&di, P->n_u_index));
+    if ((rc = upload(ctx, di, P->u_index, P->n_u_index * 8, st))) return rc;
+    h.u_idx = di;
+  }
+  if (h.elastic && P->n_s_index > 0) {
+    const long long n = P->n_s_index;
+    h.n_s = (int)n;
+    h.s_mode = P->s_mode;
+    long long *di;
+    CU(M.alloc(&di, n));
+    if ((rc = upload(ctx, di, P->s_index, n * 8, st))) return rc;
+    h.s_idx = di;
+    for (int k = 0; k < 6; ++k) {
+      const kwb_signal &sg = P->s_signal[k];
+      if (!sg.data || !h.el_s[k]) continue;
+      h.s_cols[k] = (int)sg.n_cols;
+      double *sig;
+      CU(M.alloc(&sig, sg.n_rows * sg.n_cols));
+      if ((rc = upload(ctx, sig, sg.data, sg.n_rows * sg.n_cols * 8, st))) return rc;
+      float *tab;
+      CU(M.alloc(&tab, n * sg.n_cols));
+      CU(build_source_table(tab, sig, sg.n_rows, n, sg.n_cols, nullptr, 1.0, 0, 1.0, 0, st));
+      h.s_sig[k] = tab;
+    }
+    CU(cudaStreamSynchronize(st));
   }
 
   // ---- sensor groups
@@ -1008,7 +1197,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     }
   }
   CU(cudaDeviceGetAttribute(&h.num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
-  CU(prime_attributes(h));
+  CU(h.elastic ? el_prime(h) : prime_attributes(h));
 
   // ---- device descriptor
   CU(M.alloc(&S->d_sim, 1));
@@ -1018,7 +1207,11 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   if (P->p0.count && !S->tr) {
     if ((rc = upload_grid(stage, P->p0.data))) return rc;
     CU(convert_f64_to_f32(h.p, stage, nvox, 0, st));
-    for (int a = 0; a < D; ++a) CU(launch_line_pass(S->d_sim, h, a, KWB_MODE_INIT, 0, st));
+    if (h.elastic) {
+      CU(el_init(h, st));  // every normal stress = -p0 (elastic.jl:211-215, 441-446)
+    } else {
+      for (int a = 0; a < D; ++a) CU(launch_line_pass(S->d_sim, h, a, KWB_MODE_INIT, 0, st));
+    }
   }
   CU(cudaStreamSynchronize(st));
 
@@ -1255,6 +1448,14 @@ int kwb_sim_profile(kwb_sim *S, int64_t steps, kwb_kernel_times *out) {
   };
   for (long long i = 0; i < steps && err == cudaSuccess; ++i) {
     const long long s = S->steps_done - S->t0_host;
+    if (h.elastic) {
+      elastic_step(S, s, [&](const char *nm, double bytes, auto fn) {
+        timed(slot(nm, bytes), fn);
+        return err;
+      });
+      S->steps_done++;
+      continue;
+    }
     if (S->tr) timed(slot("tr_inject", h.n_tr * 8.0), [&] { return launch_tr_inject(S->d_sim, h, s, st); });
     const double eos_rd = nv * 4.0 * (h.D + (h.c0sq ? 1 : 0) + (h.nonlinear && h.nlq ? 1 : 0) + (h.dispersion ? 2 : 0));
     for (int a : {1, 2, 0}) {

@@ -1,0 +1,303 @@
+// Elastic solver kernels: pstd_elastic_2d / pstd_elastic_3d (KWave.jl/src/solver/elastic.jl:
+// 133-366, 386-588) on the line-pass machinery of the fluid solver.
+//
+// One time step (D = 2 or 3, stresses sigma in slots xx, yy, zz, xy, xz, yz):
+//
+//   k_el_grad(x), k_el_grad(y)[, k_el_grad(z)]   w_j (+)= d/dx_d sigma_dj, staggered +
+//                                                 (elastic.jl:223-231, 448-461); one pass per
+//                                                 axis transforms the D stresses on its lines
+//   k_el_velocity                                 v_j = pml_sg,j (pml_sg,j v_j + dt/rho_sg,j w_j)
+//                                                 (:233-243, 463-476)
+//   [k_el_inject(velocity)]                       velocity sources (:245-268, 478-492)
+//   k_el_grad(x), k_el_grad(y)[, k_el_grad(z)]   w_dd = dv_d/dx_d, w_{ij} (+)= dv_i/dx_j (i != j),
+//                                                 staggered - (:270-279, 494-505)
+//   k_el_stress                                   the constitutive update with split PML, then
+//                                                 p = -trace(sigma)/D (:281-313, 507-521)
+//   [k_el_inject(stress)]                         stress sources, p refreshed at their points
+//                                                 (:315-347, 523-545)
+//   sensor gathers (kwb_kernels.cu)               record_sensor_data! on p and v (:349-356)
+//
+// Each directional derivative is the 1-D transform along its axis (the reference's full N-D
+// rfft / irfft with a multiplier that varies along one axis only), computed two real lines per
+// complex line with the shared-memory Stockham FFTs of kwb_fft.cuh.
+#include <algorithm>
+
+#include "kwb_fft.cuh"
+#include "kwb_tiles.cuh"
+
+namespace kwb {
+
+namespace {
+
+int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Column-major coordinates of voxel i.
+struct Coord {
+  int x, y, z;
+};
+__device__ __forceinline__ Coord coord_of(const SimDev &S, long long i) {
+  const int Nx = S.N[0], Ny = S.N[1];
+  Coord c;
+  const long long row = i / Nx;
+  c.x = (int)(i - row * Nx);
+  c.z = (int)(row / Ny);
+  c.y = (int)(row - (long long)c.z * Ny);
+  return c;
+}
+
+}  // namespace
+
+// Directional derivatives of g.nf fields along `axis` on one tile of 2L real lines.
+template <bool CONTIG>
+__global__ void __launch_bounds__(KWB_THREADS)
+    k_el_grad(const __grid_constant__ SimDev S, int axis, ElGrad g, long long step_s) {
+  extern __shared__ float4 smem_raw[];
+  const int N = S.N[axis];
+  const int L = S.L_line[axis];
+  const int LS = N + 1;
+  const int Nx = S.N[0];
+  float2 *X = reinterpret_cast<float2 *>(smem_raw);
+  float2 *Y = X + L * LS;
+  float2 *tw = Y + L * LS;
+  load_twiddles(tw, S.tw[axis], N);  // set-up-time table: before waiting on the previous kernel
+  KWB_STEP_KERNEL_PROLOGUE();
+  if (step_index(S, step_s) >= S.Nt) return;
+  const Tile T = CONTIG ? tile_x(S, 2 * L, blockIdx.x) : tile_yz(S, axis, 2 * L, blockIdx.x);
+  auto addr = [&](int c, int i) -> long long {
+    return CONTIG ? T.base + (long long)c * Nx + i : T.base + (long long)i * T.stride + c;
+  };
+  // element e of the tile: line l, position i (strided tiles keep neighbouring columns adjacent
+  // in a warp, so their global accesses coalesce)
+  auto decode = [&](int e, int &l, int &i) {
+    if (CONTIG) {
+      l = e / N;
+      i = e - l * N;
+    } else {
+      i = e / L;
+      l = e - i * L;
+    }
+  };
+  const int total = L * N;
+  const float2 *__restrict__ mult = g.neg ? S.gneg[axis] : S.gpos[axis];
+  for (int f = 0; f < g.nf; ++f) {
+    const float *__restrict__ src = g.src[f];
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int l, i;
+      decode(e, l, i);
+      const int ca = 2 * l, cb = 2 * l + 1;
+      const float a = ca < T.cnt ? src[addr(ca, i)] : 0.f;
+      const float b = cb < T.cnt ? src[addr(cb, i)] : 0.f;
+      X[l * LS + i] = make_float2(a, b);
+    }
+    __syncthreads();
+    float2 *R = fft_lines<false>(X, Y, L, LS, S.plan[axis], tw);
+    float2 *F = (R == X) ? Y : X;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / N, i = e - l * N;
+      R[l * LS + i] = cmul(R[l * LS + i], mult[i]);  // i k e^{+-i k d/2} / N
+    }
+    __syncthreads();
+    const float2 *Dv = fft_lines<true>(R, F, L, LS, S.plan[axis], tw);
+    float *dst = g.dst[f];
+    const bool acc = (g.acc >> f) & 1;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int l, i;
+      decode(e, l, i);
+      const float2 d = Dv[l * LS + i];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = 2 * l + h;
+        if (c >= T.cnt) continue;
+        const long long ad = addr(c, i);
+        const float dv = h ? d.y : d.x;
+        dst[ad] = acc ? dst[ad] + dv : dv;
+      }
+    }
+    __syncthreads();  // X and Y are refilled by the next field
+  }
+}
+
+// v_j = pml_sg,j (pml_sg,j v_j + dt / rho_sg,j w_j), pml = 1 - deficit; rho_sg,j the periodic
+// average of rho0 with its +1 neighbour along j (_stagger_density_{2,3}d, first_order_steps.jl:
+// 40-52).
+__global__ void __launch_bounds__(KWB_THREADS) k_el_velocity(const __grid_constant__ SimDev S, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
+  if (step_index(S, step_s) >= S.Nt) return;
+  const long long nv = S.nvox;
+  const long long plane = (long long)S.N[0] * S.N[1];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const Coord c = coord_of(S, i);
+    const int cc[3] = {c.x, c.y, c.z};
+    for (int j = 0; j < S.D; ++j) {
+      float coef = S.dt_over_rho0_s;
+      if (S.rho0) {
+        const long long step = j == 0 ? 1 : (j == 1 ? S.N[0] : plane);
+        const long long nb = cc[j] + 1 == S.N[j] ? i - (long long)cc[j] * step : i + step;
+        coef = (2.0f * S.dt) / (S.rho0[i] + S.rho0[nb]);
+      }
+      const float e = S.pml_sg_def[j][cc[j]];
+      const float v = S.u[j][i];
+      float t1 = fmaf(-e, v, v);
+      t1 = fmaf(coef, S.el_w[j][i], t1);
+      S.u[j][i] = fmaf(-e, t1, t1);
+    }
+  }
+}
+
+// Constitutive update with split PML (elastic.jl:281-313 for 2D, 507-521 for 3D), then
+// p = -trace(sigma) / D for the sensors.
+__global__ void __launch_bounds__(KWB_THREADS) k_el_stress(const __grid_constant__ SimDev S, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
+  if (step_index(S, step_s) >= S.Nt) return;
+  const long long nv = S.nvox;
+  const float dt = S.dt;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const Coord c = coord_of(S, i);
+    const float lam = S.el_lam ? S.el_lam[i] : S.el_lam_s;
+    const float mu = S.el_mu ? S.el_mu[i] : S.el_mu_s;
+    const float l2m = lam + 2.0f * mu;
+    const float ex = S.pml_def[0][c.x], ey = S.pml_def[1][c.y];
+    // pml * (pml * s + dt a), pml = 1 - e
+    auto split = [&](float s, float e, float a) {
+      float t1 = fmaf(-e, s, s);
+      t1 = fmaf(dt, a, t1);
+      return fmaf(-e, t1, t1);
+    };
+    // pml_i pml_j (s + dt a): 1 - pml_i pml_j = e_i + e_j - e_i e_j
+    auto shear = [&](float s, float ei, float ej, float a) {
+      const float eij = fmaf(-ei, ej, ei + ej);
+      const float t1 = fmaf(dt, a, s);
+      return fmaf(-eij, t1, t1);
+    };
+    if (S.D == 2) {
+      const float dxx = S.el_w[0][i], dyy = S.el_w[1][i];
+      float axx = fmaf(lam, dyy, l2m * dxx);
+      float ayy = fmaf(l2m, dyy, lam * dxx);
+      float sh = mu * S.el_w[3][i];
+      axx = fmaf(S.el_chi_p, axx, axx);
+      ayy = fmaf(S.el_chi_p, ayy, ayy);
+      sh = fmaf(S.el_chi_s, sh, sh);
+      const float sxx = split(S.el_s[0][i], ex, axx);
+      const float syy = split(S.el_s[1][i], ey, ayy);
+      S.el_s[0][i] = sxx;
+      S.el_s[1][i] = syy;
+      S.el_s[3][i] = shear(S.el_s[3][i], ex, ey, sh);
+      S.p[i] = -(sxx + syy) / 2.0f;
+    } else {
+      const float ez = S.pml_def[2][c.z];
+      const float dxx = S.el_w[0][i], dyy = S.el_w[1][i], dzz = S.el_w[2][i];
+      const float sxx = split(S.el_s[0][i], ex, fmaf(lam, dyy + dzz, l2m * dxx));
+      const float syy = split(S.el_s[1][i], ey, fmaf(lam, dxx + dzz, l2m * dyy));
+      const float szz = split(S.el_s[2][i], ez, fmaf(lam, dxx + dyy, l2m * dzz));
+      S.el_s[0][i] = sxx;
+      S.el_s[1][i] = syy;
+      S.el_s[2][i] = szz;
+      S.el_s[3][i] = shear(S.el_s[3][i], ex, ey, mu * S.el_w[3][i]);
+      S.el_s[4][i] = shear(S.el_s[4][i], ex, ez, mu * S.el_w[4][i]);
+      S.el_s[5][i] = shear(S.el_s[5][i], ey, ez, mu * S.el_w[5][i]);
+      S.p[i] = -(sxx + syy + szz) / 3.0f;
+    }
+  }
+}
+
+// Point sources: Dirichlet (mode 0) or additive; column min(t, n_cols) of each present component.
+// which 0: velocities at u_idx; which 1: stresses at s_idx, then p at those points.
+__global__ void k_el_inject(const __grid_constant__ SimDev S, int which, long long step_s) {
+  KWB_STEP_KERNEL_PROLOGUE();
+  const long long t = step_index(S, step_s);
+  if (t >= S.Nt) return;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (which == 0) {
+    if (j >= S.n_u) return;
+    const long long v = S.u_idx[j];
+    for (int d = 0; d < S.D; ++d) {
+      if (!S.u_sig[d]) continue;
+      const long long col = min(t + 1, (long long)S.u_cols[d]) - 1;
+      const float val = S.u_sig[d][col * S.n_u + j];
+      S.u[d][v] = S.u_mode == 0 ? val : S.u[d][v] + val;
+    }
+    return;
+  }
+  if (j >= S.n_s) return;
+  const long long v = S.s_idx[j];
+  for (int k = 0; k < 6; ++k) {
+    if (!S.s_sig[k] || !S.el_s[k]) continue;
+    const long long col = min(t + 1, (long long)S.s_cols[k]) - 1;
+    const float val = S.s_sig[k][col * S.n_s + j];
+    S.el_s[k][v] = S.s_mode == 0 ? val : S.el_s[k][v] + val;
+  }
+  if (S.D == 2) S.p[v] = -(S.el_s[0][v] + S.el_s[1][v]) / 2.0f;
+  else S.p[v] = -(S.el_s[0][v] + S.el_s[1][v] + S.el_s[2][v]) / 3.0f;
+}
+
+// p0: every normal stress starts at -p0 (p holds p0 in FP32).
+__global__ void k_el_init(const __grid_constant__ SimDev S) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < S.nvox; i += (long long)gridDim.x * blockDim.x) {
+    const float v = -S.p[i];
+    for (int d = 0; d < S.D; ++d) S.el_s[d][i] = v;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------------
+
+static int elementwise_grid(const SimDev &h) {
+  const long long want = cdiv(h.nvox, KWB_THREADS);
+  const long long cap = (long long)(h.num_sms > 0 ? h.num_sms : 148) * 8;
+  return (int)std::max(1LL, std::min(want, cap));
+}
+
+static cudaError_t set_smem_optin(const void *fn, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (bytes > (size_t)optin) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+}
+
+cudaError_t el_prime(const SimDev &h) {
+  cudaError_t e = set_smem_optin((const void *)k_el_grad<true>, line_pass_smem(h.N[0], h.L_line[0]));
+  size_t m = 0;
+  for (int a = 1; a < h.ndim; ++a) m = std::max(m, line_pass_smem(h.N[a], h.L_line[a]));
+  if (e == cudaSuccess) e = set_smem_optin((const void *)k_el_grad<false>, m);
+  return e;
+}
+
+cudaError_t el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
+  const int L = h.L_line[axis];
+  const size_t sm = line_pass_smem(h.N[axis], L);
+  if (axis == 0)
+    kwb_launch(k_el_grad<true>, cdiv(h.N[1], 2 * L) * h.N[2], KWB_THREADS, sm, st, h, axis, g, s);
+  else
+    kwb_launch(k_el_grad<false>, cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]), KWB_THREADS, sm, st, h,
+               axis, g, s);
+  return cudaGetLastError();
+}
+
+cudaError_t el_velocity(const SimDev &h, long long s, cudaStream_t st) {
+  kwb_launch(k_el_velocity, elementwise_grid(h), KWB_THREADS, 0, st, h, s);
+  return cudaGetLastError();
+}
+
+cudaError_t el_stress(const SimDev &h, long long s, cudaStream_t st) {
+  kwb_launch(k_el_stress, elementwise_grid(h), KWB_THREADS, 0, st, h, s);
+  return cudaGetLastError();
+}
+
+cudaError_t el_inject(const SimDev &h, int which, long long s, cudaStream_t st) {
+  const long long n = which == 0 ? h.n_u : h.n_s;
+  if (n <= 0) return cudaSuccess;
+  kwb_launch(k_el_inject, cdiv(n, 256), 256, 0, st, h, which, s);
+  return cudaGetLastError();
+}
+
+cudaError_t el_init(const SimDev &h, cudaStream_t st) {
+  k_el_init<<<elementwise_grid(h), KWB_THREADS, 0, st>>>(h);
+  return cudaGetLastError();
+}
+
+}  // namespace kwb

@@ -136,7 +136,28 @@ struct SimDev {
 
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
+
+  // Elastic solver (pstd_elastic_2d/3d).  u[d] are the velocities, p the recorded pressure
+  // -trace(sigma)/D.  el_s: stresses in the slots xx, yy, zz, xy, xz, yz (2-D: 0, 1, 3).  el_w:
+  // derivative scratch in the same slots -- first the velocity right-hand sides
+  // sum_d d/dx_d sigma_dj in 0..D-1, then dv_d/dx_d in 0..2 and the shear sums
+  // dv_i/dx_j + dv_j/dx_i in 3..5.
+  int elastic;
+  float *el_s[6];
+  float *el_w[6];
+  const float *el_lam, *el_mu;  // Lame parameters per voxel; nullptr: scalar (el_lam_s, el_mu_s)
+  float el_lam_s, el_mu_s;
+  float el_chi_p, el_chi_s;     // Kelvin-Voigt factors (2-D homogeneous medium only, else 0)
+  int s_mode;
+  int n_s;
+  int s_cols[6];
+  const float *s_sig[6];        // stress source tables [col][j]; nullptr when a component is absent
+  const long long *s_idx;       // stress source points (column-major linear indices)
+  const long long *u_idx;       // velocity source points (elastic solver)
 };
+
+// Stress slot of sigma_{dj}: the diagonal in 0..2, the pair {d, j} in 3..5 (xy, xz, yz).
+__host__ __device__ inline int kwb_stress_slot(int d, int j) { return d == j ? d : 2 + d + j; }
 
 // Launch a step kernel with programmatic stream serialization (see KWB_STEP_KERNEL_PROLOGUE).
 template <typename... K, typename... A>
@@ -206,6 +227,23 @@ bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
 void fast_plane_slot_ky(int Ny, int *ky);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
+
+// Elastic solver kernels (kwb_elastic.cu).  One gradient pass along `axis` transforms up to
+// three fields and writes (or, per bit of acc, adds) each derivative into its destination.
+struct ElGrad {
+  const float *src[3];
+  float *dst[3];
+  int nf;
+  int acc;  // bit f: dst[f] += d/dx_axis src[f]; else dst[f] = d/dx_axis src[f]
+  int neg;  // 1: staggered - (velocity gradients), 0: staggered + (stress gradients)
+};
+cudaError_t el_prime(const SimDev &h);
+cudaError_t el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
+cudaError_t el_velocity(const SimDev &h, long long s, cudaStream_t st);
+cudaError_t el_stress(const SimDev &h, long long s, cudaStream_t st);
+// which 0: velocity sources, 1: stress sources (and p at their points)
+cudaError_t el_inject(const SimDev &h, int which, long long s, cudaStream_t st);
+cudaError_t el_init(const SimDev &h, cudaStream_t st);
 
 // FP64 table builders.
 cudaError_t build_twiddles(float2 *out, int N, cudaStream_t st);

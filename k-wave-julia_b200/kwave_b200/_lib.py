@@ -73,6 +73,10 @@ class Problem(C.Structure):
         ("n_groups", C.c_int32), ("groups", C.POINTER(SensorGroup)),
         ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
         ("row_major", C.c_int32), ("axisymmetric", C.c_int32),
+        ("elastic", C.c_int32), ("cs", Field), ("has_alpha_shear", C.c_int32),
+        ("alpha_coeff_shear", C.c_double),
+        ("s_index", C.POINTER(C.c_int64)), ("n_s_index", C.c_int64), ("s_mode", C.c_int32),
+        ("s_signal", Signal * 6),
     ]
 
 

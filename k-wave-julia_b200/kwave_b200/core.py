@@ -9,6 +9,7 @@ Mirrors:
   KWaveGrid / make_time               KWave.jl/src/grid.jl:120-352
   KWaveMedium                         KWave.jl/src/medium.jl:248-341
   KWaveSource, SourceMode             KWave.jl/src/source.jl:160-230, types.jl:355
+  ElasticMedium, ElasticSource        KWave.jl/src/solver/elastic.jl:22-104
   KWaveSensor, SimulationOutput       KWave.jl/src/sensor.jl:31-87
   get_pml, get_optimal_pml_size       KWave.jl/src/pml.jl:25-121
   smooth                              KWave.jl/src/filter/filters.jl:20-73
@@ -147,6 +148,47 @@ class KWaveSource:
 
     def has_velocity_source(self) -> bool:
         return self.u_mask is not None
+
+
+@dataclass
+class ElasticMedium:
+    """``ElasticMedium(; sound_speed_compression, sound_speed_shear, density=1000.0,
+    alpha_coeff_compression, alpha_coeff_shear, alpha_power)`` (solver/elastic.jl:22-48)."""
+    sound_speed_compression: Any
+    sound_speed_shear: Any
+    density: Any = 1000.0
+    alpha_coeff_compression: Any = None
+    alpha_coeff_shear: Any = None
+    alpha_power: Optional[float] = None
+
+
+@dataclass
+class ElasticSource:
+    """``ElasticSource(; s_mask, sxx, syy, szz, sxy, sxz, syz, s_mode=Additive, u_mask, ux, uy,
+    uz, u_mode=Additive, p0)`` (solver/elastic.jl:57-104)."""
+    s_mask: Any = None
+    sxx: Any = None
+    syy: Any = None
+    szz: Any = None
+    sxy: Any = None
+    sxz: Any = None
+    syz: Any = None
+    s_mode: SourceMode = Additive
+    u_mask: Any = None
+    ux: Any = None
+    uy: Any = None
+    uz: Any = None
+    u_mode: SourceMode = Additive
+    p0: Any = None
+
+    def has_stress_source(self) -> bool:  # elastic.jl:106
+        return self.s_mask is not None
+
+    def has_velocity_source(self) -> bool:
+        return self.u_mask is not None
+
+    def has_p0(self) -> bool:
+        return self.p0 is not None
 
 
 VALID_RECORD_FIELDS = frozenset(["p", "p_max", "p_min", "p_rms", "p_final", "ux", "uy", "uz",

@@ -22,8 +22,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import KWaveB200Error, check
-from .core import (KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource, SimulationOutput,
-                   SourceMode, smooth, validate_record_fields)
+from .core import (ElasticMedium, ElasticSource, KWaveGrid, KWaveMedium, KWaveSensor, KWaveSource,
+                   SimulationOutput, SourceMode, smooth, validate_record_fields)
 
 
 def _f64(a) -> np.ndarray:
@@ -132,8 +132,12 @@ class _Built:
 
 def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
                   pml_size=20, pml_alpha=2.0, smooth_p0: bool = True, data_cast=np.float64,
-                  progress_callback=None, extra_sensors=(), axisymmetric: bool = False) -> _Built:
+                  progress_callback=None, extra_sensors=(), axisymmetric: bool = False,
+                  elastic: bool = False) -> _Built:
     """Normalise the reference's arguments into a kwb_problem (first_order.jl:311-441, 529-669).
+
+    ``elastic=True`` takes an ``ElasticMedium`` and ``ElasticSource`` for the stress-velocity
+    solver (solver/elastic.jl:133-588): p0 is not smoothed and time-reversal data is not used.
 
     ``extra_sensors`` (not in the reference API) adds further sensor groups -- (mask, record)
     pairs given as ``KWaveSensor`` or dicts -- so one solve can record different fields on
@@ -155,6 +159,9 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
     P.Nt = int(kgrid.Nt)
     P.row_major = 1  # grid arrays go over as NumPy (row-major) buffers; see _flat
     P.axisymmetric = 1 if axisymmetric else 0
+    P.elastic = 1 if elastic else 0
+    if elastic and D not in (2, 3):
+        raise TypeError("the elastic solver takes a 2D or 3D grid")
     if D == 1:
         if isinstance(pml_size, (tuple, list)) or isinstance(pml_alpha, (tuple, list)):
             raise TypeError("the 1D solver takes scalar pml_size and pml_alpha")
@@ -178,10 +185,15 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
         f.count = arr.size
         return f
 
-    P.c0 = field(medium.sound_speed, "sound_speed")
-    P.rho0 = field(medium.density if medium.density is not None else 1.0, "density")
-    P.BonA = field(medium.BonA, "BonA", optional=True)
-    if medium.is_lossless():
+    if elastic:
+        _elastic_medium(P, medium, field, D)
+    else:
+        P.c0 = field(medium.sound_speed, "sound_speed")
+        P.rho0 = field(medium.density if medium.density is not None else 1.0, "density")
+        P.BonA = field(medium.BonA, "BonA", optional=True)
+    if elastic:
+        pass
+    elif medium.is_lossless():
         P.alpha_mode = _lib.NO_ABSORPTION
     else:
         if np.ndim(medium.alpha_coeff) != 0:
@@ -197,19 +209,36 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
         P.alpha_coeff = float(medium.alpha_coeff)
         P.alpha_power = float(medium.alpha_power)
 
-    tr = sensor.is_time_reversal() and not axisymmetric  # the axisymmetric solver ignores TR data
+    # the axisymmetric and elastic solvers ignore time-reversal data
+    tr = sensor.is_time_reversal() and not axisymmetric and not elastic
     if source.p0 is not None and not tr:
         p0 = np.asarray(source.p0, dtype=np.float64)
         if p0.shape != tuple(shape):
             raise ValueError(f"p0 of shape {p0.shape} does not match the grid {tuple(shape)}")
-        do_smooth = smooth_p0 and ((D == 1 and shape[0] > 4) or (D > 1 and all(n > 1 for n in shape)))
+        do_smooth = not elastic and smooth_p0 and ((D == 1 and shape[0] > 4) or (D > 1 and all(n > 1 for n in shape)))
         if do_smooth:
             p0 = smooth(p0, restore_max=True)
         arr = b.arr(_flat(p0, shape))
         P.p0.data = _ptr_d(arr)
         P.p0.count = nvox
 
-    if source.has_pressure_source():
+    if elastic and source.has_stress_source():
+        idx = b.arr(_findall(source.s_mask, shape))
+        P.s_index = _ptr_i(idx)
+        P.n_s_index = idx.size
+        P.s_mode = int(SourceMode(source.s_mode))
+        comps = (source.sxx, source.syy, source.szz, source.sxy, source.sxz, source.syz)
+        for k, comp in enumerate(comps):
+            if comp is None or (D == 2 and k in (2, 4, 5)):  # the 2D solver reads sxx, syy, sxy
+                continue
+            sig, rows, cols = _signal(comp)
+            b.arr(sig)
+            if rows < idx.size and idx.size > 0:
+                raise IndexError(f"BoundsError: stress signal {k} has {rows} rows for {idx.size} s_mask points")
+            P.s_signal[k].data = _ptr_d(sig)
+            P.s_signal[k].n_rows = rows
+            P.s_signal[k].n_cols = cols
+    if not elastic and source.has_pressure_source():
         idx = b.arr(_findall(source.p_mask, shape))
         sig, rows, cols = _signal(source.p)
         b.arr(sig)
@@ -263,7 +292,7 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
             n_rows = int(m.shape[1])
         rec = list(sen.record)
         if ("I_avg" in rec or "I_max" in rec) and np.dtype(data_cast) == np.float32 and n_rows > 0 \
-                and m.dtype == bool:
+                and m.dtype == bool and not elastic:
             raise TypeError("MethodError: _acoustic_intensity(::Float32, ...) -- the reference records "
                             ":I_avg/:I_max only with data_cast=Float64")
         for f in rec:
@@ -295,6 +324,32 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
     return b
 
 
+def _elastic_medium(P, medium, field, D):
+    """ElasticMedium -> kwb_problem: speeds, density and the Kelvin-Voigt coefficients
+    (solver/elastic.jl:164-195)."""
+    cp, cs, rho = medium.sound_speed_compression, medium.sound_speed_shear, medium.density
+    if np.ndim(rho) == 0 and (np.ndim(cp) != 0 or np.ndim(cs) != 0):
+        raise TypeError("MethodError: a scalar density with array wave speeds is evaluated as a matrix "
+                        "power (cp^2) by the reference (solver/elastic.jl:169); give the density as an array")
+    P.c0 = field(cp, "sound_speed_compression")
+    P.cs = field(cs, "sound_speed_shear")
+    P.rho0 = field(1000.0 if rho is None else rho, "density")
+    y = medium.alpha_power
+    used = D == 2 and np.ndim(rho) == 0  # chi enters the 2D homogeneous branch only
+    for name in ("alpha_coeff_compression", "alpha_coeff_shear"):
+        a = getattr(medium, name)
+        if a is not None and used and np.ndim(a) != 0:
+            raise TypeError(f"array {name} is not supported (the homogeneous 2D branch scales by it)")
+    if y is not None:
+        P.alpha_power = float(y)
+        if medium.alpha_coeff_compression is not None and used:
+            P.alpha_mode = _lib.NO_DISPERSION  # any absorbing mode: the elastic step reads only chi
+            P.alpha_coeff = float(medium.alpha_coeff_compression)
+        if medium.alpha_coeff_shear is not None and used:
+            P.has_alpha_shear = 1
+            P.alpha_coeff_shear = float(medium.alpha_coeff_shear)
+
+
 def _alloc_outputs(ctx: Context, b: _Built, kgrid: KWaveGrid):
     lib = ctx.lib
     ng = b.problem.n_groups
@@ -322,7 +377,8 @@ def _alloc_outputs(ctx: Context, b: _Built, kgrid: KWaveGrid):
     return O, outs, arrays, pfull
 
 
-def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt_loop: int):
+def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt_loop: int,
+             post_filters: bool = True):
     dicts = []
     for g, d in enumerate(arrays):
         data = {}
@@ -333,8 +389,9 @@ def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt
     extra = dicts[1:] if sensor.mask is not None else dicts
     if pfull is not None:
         main["p_final"] = pfull
-    apply_sensor_directivity(main, sensor, kgrid)
-    apply_frequency_response(main, sensor, kgrid)
+    if post_filters:  # the elastic solvers return the recorded data as it is
+        apply_sensor_directivity(main, sensor, kgrid)
+        apply_frequency_response(main, sensor, kgrid)
     out = SimulationOutput(main)
     out.extra = extra
     return out
@@ -426,6 +483,37 @@ def kspace_first_order_as(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSo
         O, outs, arrays, pfull = _alloc_outputs(ctx, b, kgrid)
         check(ctx.lib, ctx.handle, ctx.lib.kwb_solve(ctx.handle, C.byref(b.problem), C.byref(O)))
     return _collect(b, arrays, pfull, sensor, kgrid, int(b.problem.Nt))
+
+
+def _pstd_elastic(kgrid, medium, source, sensor, pml_size, pml_alpha, progress_callback, context):
+    ctx = context or default_context()
+    b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
+                      progress_callback=progress_callback, elastic=True)
+    with ctx.lock:
+        O, outs, arrays, pfull = _alloc_outputs(ctx, b, kgrid)
+        check(ctx.lib, ctx.handle, ctx.lib.kwb_solve(ctx.handle, C.byref(b.problem), C.byref(O)))
+    return _collect(b, arrays, pfull, sensor, kgrid, int(b.problem.Nt), post_filters=False)
+
+
+def pstd_elastic_2d(kgrid: KWaveGrid, medium: ElasticMedium, source: ElasticSource, sensor: KWaveSensor,
+                    *, pml_size=20, pml_alpha=2.0, data_cast=np.float64, plot_sim: bool = False,
+                    progress_callback=None, context: Optional[Context] = None) -> SimulationOutput:
+    """2D elastic stress-velocity PSTD solve on the GPU (``pstd_elastic_2d``,
+    solver/elastic.jl:133-366); same arguments and output as the reference.  Fields and FFTs are
+    FP32; ``data_cast`` and ``plot_sim`` are accepted and ignored."""
+    if kgrid.ndim != 2:
+        raise TypeError("MethodError: pstd_elastic_2d takes a KWaveGrid2D")
+    return _pstd_elastic(kgrid, medium, source, sensor, pml_size, pml_alpha, progress_callback, context)
+
+
+def pstd_elastic_3d(kgrid: KWaveGrid, medium: ElasticMedium, source: ElasticSource, sensor: KWaveSensor,
+                    *, pml_size=10, pml_alpha=2.0, data_cast=np.float64, plot_sim: bool = False,
+                    progress_callback=None, context: Optional[Context] = None) -> SimulationOutput:
+    """3D elastic stress-velocity PSTD solve on the GPU (``pstd_elastic_3d``,
+    solver/elastic.jl:386-588); same arguments and output as the reference."""
+    if kgrid.ndim != 3:
+        raise TypeError("MethodError: pstd_elastic_3d takes a KWaveGrid3D")
+    return _pstd_elastic(kgrid, medium, source, sensor, pml_size, pml_alpha, progress_callback, context)
 
 
 class Simulation:

@@ -37,9 +37,11 @@ def test_struct_layouts_match_header():
 #include <stddef.h>
 #include "kwb.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(kwb_problem), sizeof(kwb_sensor_group),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(kwb_problem), sizeof(kwb_sensor_group),
          offsetof(kwb_problem, groups), offsetof(kwb_problem, tr), offsetof(kwb_problem, u_signal),
-         sizeof(kwb_kernel_times), sizeof(kwb_group_sizes), sizeof(kwb_outputs), offsetof(kwb_problem, p0));
+         sizeof(kwb_kernel_times), sizeof(kwb_group_sizes), sizeof(kwb_outputs), offsetof(kwb_problem, p0),
+         offsetof(kwb_problem, elastic), offsetof(kwb_problem, cs), offsetof(kwb_problem, alpha_coeff_shear),
+         offsetof(kwb_problem, s_signal));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as d:
@@ -49,7 +51,8 @@ int main(void) {
         got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     exp = [C.sizeof(L.Problem), C.sizeof(L.SensorGroup), L.Problem.groups.offset, L.Problem.tr.offset,
            L.Problem.u_signal.offset, C.sizeof(L.KernelTimes), C.sizeof(L.GroupSizes), C.sizeof(L.Outputs),
-           L.Problem.p0.offset]
+           L.Problem.p0.offset, L.Problem.elastic.offset, L.Problem.cs.offset,
+           L.Problem.alpha_coeff_shear.offset, L.Problem.s_signal.offset]
     assert got == exp
 
 
