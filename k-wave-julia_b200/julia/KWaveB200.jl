@@ -1,7 +1,7 @@
 """
     KWaveB200
 
-Runs KWave.jl's fluid k-space time stepping on an NVIDIA B200 through libkwb's C ABI
+Runs KWave.jl's k-space time stepping (fluid, axisymmetric and elastic solvers) on an NVIDIA B200 through libkwb's C ABI
 (`include/kwb.h`).  `KWaveB200.kspace_first_order` has the signature and output of
 `KWave.kspace_first_order` (KWave.jl/src/solver/first_order.jl:92-111, 287-306, 505-524):
 
@@ -75,6 +75,14 @@ struct KwbProblem
     progress_user::Ptr{Cvoid}
     row_major::Int32  # 0: Julia arrays are column-major
     axisymmetric::Int32
+    elastic::Int32
+    cs::KwbField
+    has_alpha_shear::Int32
+    alpha_coeff_shear::Float64
+    s_index::Ptr{Int64}
+    n_s_index::Int64
+    s_mode::Int32
+    s_signal::NTuple{6,KwbSignal}
 end
 struct KwbGroupSizes
     rows::NTuple{13,Int64}
@@ -127,7 +135,7 @@ end
 const _ALPHA = Dict(:no_absorption => 0, :no_dispersion => 1, :stokes => 2)
 
 function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, data_cast,
-                progress_callback; axisymmetric::Bool=false)
+                progress_callback; axisymmetric::Bool=false, elastic::Bool=false)
     (kgrid.Nt[] == 0 || kgrid.dt[] == 0) &&
         error("Time array not set. Call make_time!(kgrid, sound_speed) before running.")
     KWave.validate_record_fields(sensor)
@@ -139,22 +147,24 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
     pal = pml_alpha isa Tuple ? pml_alpha : ntuple(_ -> pml_alpha, D)
     pad3(t, v) = ntuple(i -> i <= D ? t[i] : v, 3)
 
-    lossless = KWave.is_lossless(medium)
+    lossless = elastic || KWave.is_lossless(medium)
     if !lossless && !(medium.alpha_coeff isa Real)
         error("array alpha_coeff is not supported")          # T(absorb_tau) raises in the reference
     end
-    tr = KWave.is_time_reversal(sensor) && !axisymmetric  # the axisymmetric solver ignores TR data
+    # the axisymmetric and elastic solvers ignore time-reversal data
+    tr = KWave.is_time_reversal(sensor) && !axisymmetric && !elastic
     p0 = KwbField(C_NULL, 0)
     if KWave.has_p0(source) && !tr
         q = Float64.(Array(source.p0))
-        if smooth_p0 && ((D == 1 && dims[1] > 4) || (D > 1 && all(>(1), dims)))
+        if !elastic && smooth_p0 && ((D == 1 && dims[1] > 4) || (D > 1 && all(>(1), dims)))
             q = KWave.smooth(q; restore_max=true)
         end
         p0 = field(q, keep)
     end
-    p_idx = KWave.has_pressure_source(source) ? indices(source.p_mask, keep) : Int64[]
+    has_p = !elastic && KWave.has_pressure_source(source)
+    p_idx = has_p ? indices(source.p_mask, keep) : Int64[]
     u_idx = KWave.has_velocity_source(source) ? indices(source.u_mask, keep) : Int64[]
-    psig = KWave.has_pressure_source(source) ? signal(source.p, keep) : KwbSignal(C_NULL, 0, 0)
+    psig = has_p ? signal(source.p, keep) : KwbSignal(C_NULL, 0, 0)
     usig = (signal(source.ux, keep), D > 1 ? signal(source.uy, keep) : KwbSignal(C_NULL, 0, 0),
             D > 2 ? signal(source.uz, keep) : KwbSignal(C_NULL, 0, 0))
 
@@ -167,7 +177,7 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
             counts[REC[f] + 1] += 1
         end
         if (:I_avg in sensor.record || :I_max in sensor.record) && data_cast == Float32 &&
-           sensor.mask isa AbstractArray{Bool}
+           sensor.mask isa AbstractArray{Bool} && !elastic
             throw(MethodError(KWave._acoustic_intensity, (0.0f0,)))
         end
         if sensor.mask isa AbstractArray{Bool}
@@ -191,16 +201,39 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
         cb = Base.unsafe_convert(Ptr{Cvoid}, cfn)
     end
 
+    nosig = KwbSignal(C_NULL, 0, 0)
+    if elastic
+        # ElasticMedium / ElasticSource (solver/elastic.jl:22-104); chi enters the 2D branch with a
+        # scalar density only (elastic.jl:177-195, 282-295)
+        used = D == 2 && medium.density isa Real
+        y = medium.alpha_power
+        absorb_p = used && y !== nothing && medium.alpha_coeff_compression !== nothing
+        absorb_s = used && y !== nothing && medium.alpha_coeff_shear !== nothing
+        c0f, rhof, bonaf = field(medium.sound_speed_compression, keep), field(medium.density, keep), KwbField(C_NULL, 0)
+        amode, acoef, apow = absorb_p ? 1 : 0, absorb_p ? Float64(medium.alpha_coeff_compression) : 0.0,
+                             y === nothing ? 0.0 : Float64(y)
+        csf = field(medium.sound_speed_shear, keep)
+        ashear = absorb_s ? Float64(medium.alpha_coeff_shear) : 0.0
+        s_idx = KWave.has_stress_source(source) ? indices(source.s_mask, keep) : Int64[]
+        comps = (source.sxx, source.syy, D > 2 ? source.szz : nothing, source.sxy,
+                 D > 2 ? source.sxz : nothing, D > 2 ? source.syz : nothing)
+        ssig = ntuple(k -> isempty(s_idx) ? nosig : signal(comps[k], keep), 6)
+        smode = Int32(Int(source.s_mode))
+    else
+        c0f, rhof, bonaf = field(medium.sound_speed, keep), field(medium.density, keep), field(medium.BonA, keep)
+        amode = lossless ? 0 : _ALPHA[medium.alpha_mode]
+        acoef = lossless ? 0.0 : Float64(medium.alpha_coeff)
+        apow = lossless ? 0.0 : Float64(medium.alpha_power)
+        csf, absorb_s, ashear, s_idx, ssig, smode = KwbField(C_NULL, 0), false, 0.0, Int64[], ntuple(_ -> nosig, 6), Int32(0)
+    end
     P = Ref(KwbProblem(Int32(D), pad3(dims, 1), pad3(ds, 1.0), kgrid.dt[], kgrid.Nt[],
                        pad3(psz, 0), pad3(Float64.(pal), 0.0),
-                       field(medium.sound_speed, keep), field(medium.density, keep),
-                       field(medium.BonA, keep),
-                       lossless ? 0 : _ALPHA[medium.alpha_mode],
-                       lossless ? 0.0 : Float64(medium.alpha_coeff),
-                       lossless ? 0.0 : Float64(medium.alpha_power), p0,
-                       isempty(p_idx) ? C_NULL : pointer(p_idx), length(p_idx), Int32(Int(source.p_mode)), psig,
+                       c0f, rhof, bonaf, amode, acoef, apow, p0,
+                       isempty(p_idx) ? C_NULL : pointer(p_idx), length(p_idx), has_p ? Int32(Int(source.p_mode)) : Int32(1), psig,
                        isempty(u_idx) ? C_NULL : pointer(u_idx), length(u_idx), Int32(Int(source.u_mode)), usig,
-                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL, Int32(0), Int32(axisymmetric)))
+                       trs, length(groups), isempty(groups) ? C_NULL : pointer(groups), cb, C_NULL, Int32(0), Int32(axisymmetric),
+                       Int32(elastic), csf, Int32(absorb_s), ashear,
+                       isempty(s_idx) ? C_NULL : pointer(s_idx), length(s_idx), smode, ssig))
     ctx = context()
     GC.@preserve keep begin
         sizes = Vector{KwbGroupSizes}(undef, max(length(groups), 1))
@@ -229,8 +262,10 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
         kgrid.Nt[] = size(sensor.time_reversal_boundary_data, 2)   # first_order.jl:430-431
         data[:p_final] = pfull
     end
-    KWave.apply_sensor_directivity!(data, sensor, kgrid)            # host post-filters, as the
-    KWave.apply_frequency_response!(data, sensor, kgrid)            # reference runs them
+    if !elastic  # the elastic solvers return the recorded data as it is
+        KWave.apply_sensor_directivity!(data, sensor, kgrid)        # host post-filters, as the
+        KWave.apply_frequency_response!(data, sensor, kgrid)        # reference runs them
+    end
     return KWave.SimulationOutput(data)
 end
 
@@ -267,6 +302,34 @@ function kspace_first_order_as(kgrid::KWave.KWaveGrid2D, medium::KWave.KWaveMedi
                                record_movie=nothing, progress_callback=nothing) where {T<:AbstractFloat}
     return _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, T, progress_callback;
                   axisymmetric=true)
+end
+
+"""
+    pstd_elastic_2d(kgrid, medium, source, sensor; kwargs...) -> SimulationOutput
+
+Same arguments and output as `KWave.pstd_elastic_2d` (solver/elastic.jl:133-366); the time loop
+runs on the GPU.  A scalar density with array wave speeds is rejected (the reference evaluates
+`cp^2` as a matrix power there).
+"""
+function pstd_elastic_2d(kgrid::KWave.KWaveGrid2D, medium::KWave.ElasticMedium,
+                         source::KWave.ElasticSource, sensor::KWave.KWaveSensor;
+                         pml_size=20, pml_alpha=2.0, data_cast::Type{T}=Float64, plot_sim::Bool=false,
+                         progress_callback=nothing) where {T<:AbstractFloat}
+    return _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, false, T, progress_callback;
+                  elastic=true)
+end
+
+"""
+    pstd_elastic_3d(kgrid, medium, source, sensor; kwargs...) -> SimulationOutput
+
+Same arguments and output as `KWave.pstd_elastic_3d` (solver/elastic.jl:386-588).
+"""
+function pstd_elastic_3d(kgrid::KWave.KWaveGrid3D, medium::KWave.ElasticMedium,
+                         source::KWave.ElasticSource, sensor::KWave.KWaveSensor;
+                         pml_size=10, pml_alpha=2.0, data_cast::Type{T}=Float64, plot_sim::Bool=false,
+                         progress_callback=nothing) where {T<:AbstractFloat}
+    return _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, false, T, progress_callback;
+                  elastic=true)
 end
 
 end # module

@@ -79,3 +79,25 @@ def test_missing_library_fails_loudly(tmp_path):
             L.load_library(str(tmp_path / "libkwb.so"))
     finally:
         L._lib = saved
+
+
+def test_julia_problem_struct_matches_header():
+    """The Julia shim's KwbProblem (no Julia here to run it) lists the header's fields, in order,
+    with the same C sizes."""
+    import re
+    import kwave_b200._lib as L
+    src = open(os.path.join(ROOT, "k-wave-julia_b200", "julia", "KWaveB200.jl")).read()
+    body = re.search(r"struct KwbProblem\n(.*?)\nend\n", src, re.S).group(1)
+    jl = [(m.group(1), m.group(2)) for m in re.finditer(r"^\s*(\w+)::([\w{},]+)", body, re.M)]
+    size = {"Int32": 4, "Int64": 8, "Float64": 8, "UInt32": 4, "KwbField": 16, "KwbSignal": 24}
+
+    def jl_size(t):
+        m = re.fullmatch(r"NTuple\{(\d+),(\w+)\}", t)
+        if m:
+            return int(m.group(1)) * size[m.group(2)]
+        return 8 if t.startswith("Ptr") else size[t]
+
+    names = [n for n, _ in L.Problem._fields_]
+    assert [n for n, _ in jl] == names
+    for (n, t), (_, ct) in zip(jl, L.Problem._fields_):
+        assert jl_size(t) == C.sizeof(ct), (n, t)
