@@ -256,6 +256,51 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def elastic_bench(ctx, n=256, steps=200, warmup=5, cpu=True):
+    """The elastic solver (pstd_elastic_3d) on the n^3 heterogeneous elastic workload: device-timed
+    steps (CUDA events, CUDA-graph chunks), per-kernel shares and algorithmic bytes, and the FP64
+    oracle on the host cores for a 2-step prefix of the same workload."""
+    import kwave_b200 as kb
+    from kwave_b200 import workloads
+    case = workloads.elastic3d(n)
+    g, m, s, sen, kw = case.to_api()
+    sim = kb.Simulation(g, m, s, sen, context=ctx, **kw)
+    sim.advance_timed(warmup)
+    ms = sim.advance_timed(steps)
+    sim.close()
+    prof_sim = kb.Simulation(g, m, s, sen, context=ctx, **kw)
+    prof_sim.advance(warmup)
+    prof = prof_sim.profile(20)
+    prof_sim.close()
+    tot = sum(k["total_ms"] for k in prof)
+    steps_prof = 20
+    bytes_step = sum(k["bytes_per_launch"] * k["launches"] for k in prof) / steps_prof
+    peak, peak_kind = peaks()
+    ms_step = ms / steps
+    out = {"workload": case.name, "grid": list(case.N), "steps": steps, "warmup": warmup,
+           "ms_per_step": ms_step, "value": case.voxels / (ms_step / 1e3) / 1e9, "unit": UNIT,
+           "bytes_per_voxel_step": bytes_step / case.voxels,
+           "achieved_GBps": bytes_step / (ms_step / 1e3) / 1e9, "peak": peak,
+           "frac": bytes_step / (ms_step / 1e3) / 1e9 / peak, "peak_kind": f"{peak_kind} copy bandwidth",
+           "kernels": {k["name"]: {"avg_us": 1e3 * k["total_ms"] / k["launches"], "share": k["total_ms"] / tot,
+                                   "launches_per_step": k["launches"] / steps_prof} for k in prof}}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import kwave_ref as K
+        args = []
+        for nn, dd in zip(case.N, case.d):
+            args += [nn, dd]
+        og = K.KWaveGrid(*args)
+        og.dt, og.Nt = case.dt, case.Nt
+        t0 = time.perf_counter()
+        K.pstd_elastic_3d(og, K.ElasticMedium(**case.medium), K.ElasticSource(**case.source),
+                          K.KWaveSensor(**case.sensor), pml_size=case.pml_size, max_steps=2)
+        el = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": case.voxels * 2 / el / 1e9, "unit": UNIT, "cores": os.cpu_count(),
+                               "kind": "port", "sample": f"FP64 oracle, first 2 time steps incl. set-up ({el:.1f} s)"}
+    return out
+
+
 def batch_bench(ctx, n_sims=64, max_running=64, one_at_a_time=True):
     """Batch workload: n mixed-size 2D simulations, batched (continuous batching, all submitted at once)
     against one-at-a-time blocking solves of the same prepared problems.  Sims/s is measured
@@ -367,6 +412,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched mixed-size 2D measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the Poisson serving measurement")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT-based comparator")
+    ap.add_argument("--no-elastic", action="store_true", help="skip the elastic-solver measurement")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -429,6 +475,10 @@ def main():
     batch = None if args.no_batch else batch_bench(ctx)
     serve = None if args.no_serve else serving_bench(ctx)
 
+    elastic = None
+    if not args.no_elastic:
+        elastic = elastic_bench(ctx, cpu=(rank == 0 and world == 1 and not args.no_cpu))
+
     comparators = None
     if rank == 0 and world == 1 and not args.no_cufft:
         comparators = {"cufft_reference_step": cufft_comparator(case)}
@@ -462,6 +512,7 @@ def main():
             "serving": serve,
             "cpu_baseline": cpu,
             "comparators": comparators,
+            "elastic": elastic,
             "clocks": clk.summary(),
             "gpu_launches": info["launches_per_step"] * K + (K // 32),
         }

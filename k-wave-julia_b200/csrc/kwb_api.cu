@@ -750,7 +750,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (tv && strcmp(tv, "big") == 0) h.tile_override = 0;
     if (tv && strcmp(tv, "mid") == 0) h.tile_override = 1;
     if (tv && strcmp(tv, "small") == 0) h.tile_override = 2;
-    if (h.elastic) h.fast = 0;  // the elastic passes run on the generic line FFTs
+    if (h.elastic) h.fast &= 1;  // elastic: line passes only (no equation of state)
   }
 
   // ---- tile shapes and FFT plans

@@ -19,7 +19,8 @@
 //
 // Each directional derivative is the 1-D transform along its axis (the reference's full N-D
 // rfft / irfft with a multiplier that varies along one axis only), computed two real lines per
-// complex line with the shared-memory Stockham FFTs of kwb_fft.cuh.
+// complex line: power-of-two lines on the register FFTs of kwb_fast.cu (k_el_grad_fast), other
+// lengths on the shared-memory Stockham FFTs of kwb_fft.cuh (k_el_grad below).
 #include <algorithm>
 
 #include "kwb_fft.cuh"
@@ -50,7 +51,7 @@ __device__ __forceinline__ Coord coord_of(const SimDev &S, long long i) {
 // Directional derivatives of g.nf fields along `axis` on one tile of 2L real lines.
 template <bool CONTIG>
 __global__ void __launch_bounds__(KWB_THREADS)
-    k_el_grad(const __grid_constant__ SimDev S, int axis, ElGrad g, long long step_s) {
+    k_el_grad(const __grid_constant__ SimDev S, int axis, const __grid_constant__ ElGrad g, long long step_s) {
   extern __shared__ float4 smem_raw[];
   const int N = S.N[axis];
   const int L = S.L_line[axis];
@@ -259,15 +260,24 @@ static cudaError_t set_smem_optin(const void *fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
 }
 
+// Register-FFT passes serve power-of-two lines (strided ones need Nx a multiple of 4 for their
+// 16-byte staging); every other length runs on the Stockham kernel above.
+static bool el_fast(const SimDev &h, int axis) {
+  return (h.fast & 1) && fast_size(h.N[axis]) && (axis == 0 || h.N[0] % 4 == 0);
+}
+
 cudaError_t el_prime(const SimDev &h) {
   cudaError_t e = set_smem_optin((const void *)k_el_grad<true>, line_pass_smem(h.N[0], h.L_line[0]));
   size_t m = 0;
   for (int a = 1; a < h.ndim; ++a) m = std::max(m, line_pass_smem(h.N[a], h.L_line[a]));
   if (e == cudaSuccess) e = set_smem_optin((const void *)k_el_grad<false>, m);
+  for (int a = 0; a < h.ndim && e == cudaSuccess; ++a)
+    if (el_fast(h, a)) e = fast_prime(h.N[a]);
   return e;
 }
 
 cudaError_t el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
+  if (el_fast(h, axis)) return fast_el_grad(h, axis, g, s, st);
   const int L = h.L_line[axis];
   const size_t sm = line_pass_smem(h.N[axis], L);
   if (axis == 0)

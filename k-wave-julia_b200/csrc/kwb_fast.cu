@@ -1200,11 +1200,17 @@ struct LinePolicy<1024> {
   static constexpr int THREADS = 512, MINB = 1;
 };
 
+// elastic gradient pass (defined below), primed with the line-pass variants of the same tiles
+template <class F, bool CONTIG, int LT, int MINB>
+__global__ void __launch_bounds__(LT * F::G, MINB)
+    k_el_grad_fast(const __grid_constant__ SimDev S, int axis, const __grid_constant__ ElGrad g, long long step_s);
+
 template <int N, bool C, int LT>
 static cudaError_t prime_line_variant() {
   using P = LinePolicy<N>;
   using F = typename P::template F<C>;
   cudaError_t e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, false>, pline_smem<F>(LT));
+  if (e == cudaSuccess) e = raise_smem((const void *)k_el_grad_fast<F, C, LT, P::MINB>, pline_smem<F>(LT));
   if constexpr (C) {
     if (e == cudaSuccess) e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, true>, pline_smem<F>(LT));
   }
@@ -1369,6 +1375,164 @@ static int plane_clusters_per_device() {
   }
   return n;
 }
+
+// ------------------------------------------------------------------------------------------
+// elastic solver: directional derivatives of up to three fields in one line pass (the step
+// sequence and the generic shared-memory version are in kwb_elastic.cu)
+// ------------------------------------------------------------------------------------------
+
+// The fields go through the two staging slots in turn: field f + 1 lands while field f is
+// transformed, and field f + 2 takes field f's slot once every thread holds field f.  Each
+// derivative is written, or added to the destination (bit f of g.acc).
+template <class F, bool CONTIG, int LT, int MINB>
+__global__ void __launch_bounds__(LT * F::G, MINB)
+    k_el_grad_fast(const __grid_constant__ SimDev S, int axis, const __grid_constant__ ElGrad g, long long step_s) {
+  constexpr int E = F::E, G = F::G;
+  constexpr int RP = G + 1, LP = F::LP;
+  constexpr int L = LT;
+  extern __shared__ float4 smem_raw[];
+  float2 *sm = reinterpret_cast<float2 *>(smem_raw);
+  float2 *tw2 = sm + L * LP;
+  float2 *gp2 = tw2 + F::TW;
+  float2 *gn2 = gp2 + E * RP;
+  build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
+  KWB_STEP_KERNEL_PROLOGUE();
+  if (*S.t0 + step_s >= S.Nt) return;
+  const int tid = threadIdx.x;
+  const int tt = CONTIG ? tid % G : tid / L;
+  const int l = CONTIG ? tid / G : tid % L;
+  constexpr int N = E * G, THREADS = LT * G;
+  const int Nx = S.N[0];
+  long long base;
+  int cnt;
+  int st32 = 1;
+  if (CONTIG) {
+    const int Ny = S.N[1];
+    const int rows = 2 * L, tpp = (Ny + rows - 1) / rows;
+    const int z = blockIdx.x / tpp, y0 = (blockIdx.x - z * tpp) * rows;
+    cnt = min(rows, Ny - y0);
+    base = ((long long)z * Ny + y0) * Nx;
+  } else {
+    const int cols = 2 * L, tpp = (Nx + cols - 1) / cols;
+    const int o = blockIdx.x / tpp, x0 = (blockIdx.x - o * tpp) * cols;
+    cnt = min(cols, Nx - x0);
+    if (axis == 1) {
+      base = (long long)o * Nx * S.N[1] + x0;
+      st32 = Nx;
+    } else {
+      base = (long long)o * Nx + x0;
+      st32 = Nx * S.N[1];
+    }
+  }
+  const bool va = 2 * l < cnt, vb = 2 * l + 1 < cnt;
+  auto off = [&](int c, int i) -> int { return CONTIG ? c * Nx + i : i * st32 + c; };
+  float *st0 = reinterpret_cast<float *>(reinterpret_cast<char *>(smem_raw) + pline_offset<F>(L));
+  float *st1 = st0 + 2 * L * N;
+  auto stage = [&](float *dst, const float *f) {
+    const float *fb = f + base;
+    if (CONTIG) {
+      constexpr int CH = 2 * L * N / 4, PER = (CH + THREADS - 1) / THREADS;
+      const int chunks = cnt * N / 4;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int q = tid + k * THREADS;
+        if (q < chunks) cp_async16(dst + 4 * q, fb + 4 * q, 16);
+      }
+    } else {
+      constexpr int CPR = (2 * L) / 4;
+      static_assert(THREADS % CPR == 0 && (CPR * N) % THREADS == 0, "strided staging");
+      constexpr int RSTEP = THREADS / CPR, PER = CPR * N / THREADS;
+      const int ch = tid % CPR, i0 = tid / CPR;
+      const int valid = min(4, cnt - 4 * ch);
+      const int bytes = valid > 0 ? 4 * valid : 0;
+      float *d0 = dst + i0 * 2 * L + 4 * ch;
+      const float *s0 = fb + i0 * st32 + 4 * ch;
+      const int sstep = RSTEP * st32;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) cp_async16(d0 + k * RSTEP * 2 * L, s0 + k * sstep, bytes);
+    }
+    cp_async_commit();
+  };
+  auto staged = [&](const float *st, int i) -> float2 {
+    if (CONTIG) return make_float2(va ? st[(2 * l) * N + i] : 0.f, vb ? st[(2 * l + 1) * N + i] : 0.f);
+    return *reinterpret_cast<const float2 *>(st + i * 2 * L + 2 * l);
+  };
+  // the destination as this kernel may already have written it: ordinary (coherent) loads
+  auto load_cur = [&](const float *f, int i) -> float2 {
+    const float *fb = f + base;
+    if (!CONTIG) return vb ? *reinterpret_cast<const float2 *>(fb + off(2 * l, i)) : make_float2(0.f, 0.f);
+    return make_float2(va ? fb[off(2 * l, i)] : 0.f, vb ? fb[off(2 * l + 1, i)] : 0.f);
+  };
+  auto store_pair = [&](float *f, int i, float2 v) {
+    float *fb = f + base;
+    if (!CONTIG) {
+      if (vb) *reinterpret_cast<float2 *>(fb + off(2 * l, i)) = v;
+      return;
+    }
+    if (va) fb[off(2 * l, i)] = v.x;
+    if (vb) fb[off(2 * l + 1, i)] = v.y;
+  };
+  const float2 *mul = g.neg ? gn2 : gp2;
+  stage(st0, g.src[0]);
+  if (g.nf > 1) stage(st1, g.src[1]);
+  else cp_async_commit();
+  float2 *xs = sm + l * LP;
+  for (int f = 0; f < g.nf; ++f) {
+    float *slot = (f & 1) ? st1 : st0;
+    if (f == g.nf - 1) cp_async_wait<0>();
+    else cp_async_wait<1>();
+    __syncthreads();  // field f has landed for every thread; the tables too
+    float2 v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) v[r] = staged(slot, tt + G * r);
+    if (f + 2 < g.nf) {
+      __syncthreads();  // every thread holds field f
+      stage(slot, g.src[f + 2]);
+    }
+    F::fwd(v, xs, tw2, tt);
+#pragma unroll
+    for (int q = 0; q < E; ++q) v[q] = cmul(v[q], mul[q * RP + tt]);
+    F::inv(v, xs, tw2, tt);
+    float *dst = g.dst[f];
+    const bool acc = (g.acc >> f) & 1;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+      const int i = tt + G * r;
+      store_pair(dst, i, acc ? padd(load_cur(dst, i), v[r]) : v[r]);
+    }
+  }
+}
+
+template <int N, int LT>
+static void el_go(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
+  using P = LinePolicy<N>;
+  if (axis == 0) {
+    using F = typename P::template F<true>;
+    kwb_launch(k_el_grad_fast<F, true, LT, P::MINB>, cdiv(h.N[1], 2 * LT) * h.N[2], LT * F::G, pline_smem<F>(LT),
+               st, h, axis, g, s);
+  } else {
+    using F = typename P::template F<false>;
+    kwb_launch(k_el_grad_fast<F, false, LT, P::MINB>, cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]),
+               LT * F::G, pline_smem<F>(LT), st, h, axis, g, s);
+  }
+}
+
+template <int N>
+static cudaError_t launch_el_n(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
+  using P = LinePolicy<N>;
+  constexpr int G = P::template F<true>::G;
+  constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
+  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * BIG) * h.N[2]
+                                    : (long long)cdiv(h.N[0], 2 * BIG) * (axis == 1 ? h.N[2] : h.N[1]);
+  switch (tile_variant(h, tiles)) {
+    case 1: el_go<N, MID>(h, axis, g, s, st); break;
+    case 2: el_go<N, SMALL>(h, axis, g, s, st); break;
+    default: el_go<N, BIG>(h, axis, g, s, st); break;
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace fast
 
 bool fast_plane_size(int Ny, int Nz) { return Ny == 256 && Nz == 256; }
@@ -1414,6 +1578,9 @@ cudaError_t fast_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s
 }
 cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s, cudaStream_t st) {
   KWB_LINE_SWITCH(h.N[axis], launch_spec_n, (d_sim, h, axis, op, s, st))
+}
+cudaError_t fast_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
+  KWB_LINE_SWITCH(h.N[axis], launch_el_n, (h, axis, g, s, st))
 }
 
 }  // namespace kwb

@@ -244,6 +244,8 @@ cudaError_t el_stress(const SimDev &h, long long s, cudaStream_t st);
 // which 0: velocity sources, 1: stress sources (and p at their points)
 cudaError_t el_inject(const SimDev &h, int which, long long s, cudaStream_t st);
 cudaError_t el_init(const SimDev &h, cudaStream_t st);
+// Register-FFT gradient pass (kwb_fast.cu) for line lengths 64 ... 1024.
+cudaError_t fast_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
 
 // FP64 table builders.
 cudaError_t build_twiddles(float2 *out, int N, cudaStream_t st);

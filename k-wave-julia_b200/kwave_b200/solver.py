@@ -523,8 +523,11 @@ class Simulation:
                  smooth_p0=True, extra_sensors=(), context: Optional[Context] = None):
         self.ctx = context or default_context()
         self.kgrid, self.sensor = kgrid, sensor
+        # an ElasticMedium selects the elastic solver (pstd_elastic_2d/3d)
+        self.elastic = isinstance(medium, ElasticMedium)
         self.b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size,
-                               pml_alpha=pml_alpha, smooth_p0=smooth_p0, extra_sensors=extra_sensors)
+                               pml_alpha=pml_alpha, smooth_p0=smooth_p0, extra_sensors=extra_sensors,
+                               elastic=self.elastic)
         self.Nt = int(self.b.problem.tr.n_cols if self.b.problem.tr.data else self.b.problem.Nt)
         h = C.c_void_p()
         with self.ctx.lock:
@@ -559,7 +562,7 @@ class Simulation:
     def outputs(self) -> SimulationOutput:
         O, outs, arrays, pfull = _alloc_outputs(self.ctx, self.b, self.kgrid)
         self._chk(self.ctx.lib.kwb_sim_read_outputs(self.handle, C.byref(O)))
-        return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt)
+        return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt, post_filters=not self.elastic)
 
     def profile(self, steps: int) -> list:
         kt = _lib.KernelTimes()

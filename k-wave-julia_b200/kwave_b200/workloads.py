@@ -15,6 +15,8 @@ reference API with the same field names.
       xy plane p + volume p_max
   c4  64 mixed-size 2D heterogeneous absorbing simulations with tone-burst point/disc sources
   c5  Poisson serving stream (70 % 2D 256-1024, 30 % 3D 64^3-192^3)
+  elastic3d  256^3 heterogeneous elastic solid (pstd_elastic_3d), p0 ball + sxx point source,
+      xy plane p
 """
 
 from __future__ import annotations
@@ -223,3 +225,65 @@ def c5_request(i: int, seed: int = 5005, nt_range=(500, 1500)):
                 dict(p_mask=p_mask, p=sig, p_mode=Additive),
                 dict(mask=sensor, record=["p"]), pml_size=10 if D == 3 else 20, seed=seed)
     return case
+
+
+@dataclass
+class ElasticCase:
+    """An elastic-solver workload (pstd_elastic_2d/3d): medium and source keyword dicts for
+    ``ElasticMedium`` / ``ElasticSource``."""
+    name: str
+    N: tuple
+    d: tuple
+    dt: float
+    Nt: int
+    medium: dict
+    source: dict
+    sensor: dict
+    pml_size: Any = 10
+    pml_alpha: Any = 2.0
+    seed: Optional[int] = None
+
+    @property
+    def voxels(self) -> int:
+        return int(np.prod(self.N))
+
+    def to_api(self):
+        """(kgrid, medium, source, sensor, kwargs) in this package's types."""
+        from .core import ElasticMedium, ElasticSource
+        args = []
+        for n, dd in zip(self.N, self.d):
+            args += [n, dd]
+        g = KWaveGrid(*args)
+        g.dt = self.dt
+        g.Nt = self.Nt
+        g.t_array = np.arange(self.Nt) * self.dt
+        kw = dict(pml_size=self.pml_size, pml_alpha=self.pml_alpha)
+        return g, ElasticMedium(**self.medium), ElasticSource(**self.source), KWaveSensor(**self.sensor), kw
+
+
+def elastic3d(n: int = 256, Nt: int = 1000, seed: int = 6006, pml: int = 10) -> ElasticCase:
+    """n^3 heterogeneous elastic solid (cp 2600-3200, cs 1100-1600 m/s, rho 1600-2100 kg/m^3,
+    Gaussian random fields of sigma 5 px at 256), a p0 ball of radius 6 px at the centre and a
+    3 MHz sxx tone burst at one point; the sensor records p on the xy plane z = n/2."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shape = (n, n, n)
+    s = 5.0 * n / 256
+    cp = gaussian_random_field(rng, shape, s, 2600.0, 3200.0)
+    cs = gaussian_random_field(rng, shape, s, 1100.0, 1600.0)
+    rho = gaussian_random_field(rng, shape, s, 1600.0, 2100.0)
+    dx = 2e-4
+    dt = 0.3 * dx / 3200.0
+    mid = n // 2
+    p0 = np.zeros(shape)
+    p0[make_ball(n, n, n, mid, mid, mid, 6 * n / 256)] = 1e5
+    s_mask = np.zeros(shape, dtype=bool)
+    s_mask[n // 4, mid - 1, mid - 1] = True
+    tb = 1e4 * tone_burst(1 / dt, 3e6, 3)
+    sig = np.zeros((1, Nt))
+    sig[0, : min(len(tb), Nt)] = tb[: min(len(tb), Nt)]
+    plane = np.zeros(shape, dtype=bool)
+    plane[:, :, mid - 1] = True
+    return ElasticCase(f"elastic3d_{n}^3_heterogeneous", shape, (dx, dx, dx), dt, Nt,
+                       dict(sound_speed_compression=cp, sound_speed_shear=cs, density=rho),
+                       dict(p0=p0, s_mask=s_mask, sxx=sig),
+                       dict(mask=plane, record=["p"]), pml_size=pml, seed=seed)

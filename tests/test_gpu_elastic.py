@@ -234,3 +234,27 @@ def test_rejections(kb):
         kb.pstd_elastic_2d(g, kb.ElasticMedium(np.full((32, 32), 3000.0), 1500.0, 1800.0), kb.ElasticSource(), sen)
     with pytest.raises(TypeError):
         kb.pstd_elastic_3d(g, kb.ElasticMedium(3000.0, 1500.0, 1800.0), kb.ElasticSource(), sen)
+
+
+def test_register_and_stockham_paths_agree(kb, monkeypatch):
+    """Power-of-two lines run on the register-FFT gradient pass; KWB_FFT_PATH=generic forces the
+    shared-memory Stockham pass.  Both match the oracle and each other."""
+    from kwave_b200.workloads import elastic3d
+    case = elastic3d(64, Nt=60)
+    g, m, s, sen, kw = case.to_api()
+    outs = {}
+    for path in ("default", "generic"):
+        if path == "generic":
+            monkeypatch.setenv("KWB_FFT_PATH", "generic")
+        outs[path] = kb.pstd_elastic_3d(g, m, s, sen, **kw)
+    import kwave_ref as K
+    args = []
+    for n, d in zip(case.N, case.d):
+        args += [n, d]
+    og = K.KWaveGrid(*args)
+    og.dt, og.Nt = case.dt, case.Nt
+    ref = K.pstd_elastic_3d(og, K.ElasticMedium(**case.medium), K.ElasticSource(**case.source),
+                            K.KWaveSensor(**case.sensor), pml_size=case.pml_size)
+    for path in outs:
+        assert_parity(outs[path], ref, TOL_L2, TOL_MAX)
+    assert_parity(outs["default"], outs["generic"], 1e-5, 1e-4)
