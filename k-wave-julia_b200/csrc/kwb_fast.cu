@@ -1492,13 +1492,17 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     F::fwd(v, xs, tw2, tt);
 #pragma unroll
     for (int q = 0; q < E; ++q) v[q] = cmul(v[q], mul[q * RP + tt]);
-    F::inv(v, xs, tw2, tt);
     float *dst = g.dst[f];
     const bool acc = (g.acc >> f) & 1;
+    // the running sum is loaded while the inverse transform runs
+    float2 prev[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) prev[r] = acc ? load_cur(dst, tt + G * r) : make_float2(0.f, 0.f);
+    F::inv(v, xs, tw2, tt);
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const int i = tt + G * r;
-      store_pair(dst, i, acc ? padd(load_cur(dst, i), v[r]) : v[r]);
+      store_pair(dst, i, acc ? padd(prev[r], v[r]) : v[r]);
     }
   }
 }
