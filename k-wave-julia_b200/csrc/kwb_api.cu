@@ -422,9 +422,31 @@ void build_csr(const int64_t *idx, long long n, const int N[3], int a, std::vect
   for (long long j = 0; j < n; ++j) ent[fill[tmp[j].line]++] = tmp[j];
 }
 
+// Host -> device.  Large arrays go through the context's pinned buffer in halves: host threads
+// copy chunk c into one half while the DMA of chunk c - 1 drains the other, instead of the
+// driver's single-threaded staging of pageable memory.  Returns with both halves idle.
 int upload(kwb_ctx *ctx, void *dst, const void *src, size_t bytes, cudaStream_t st) {
   if (bytes == 0) return KWB_OK;
-  CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  const size_t half = kPinFloats * sizeof(float);
+  if (bytes < (size_t)8 << 20) {
+    CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return KWB_OK;
+  }
+  if (!ctx->pin) {
+    CU(cudaMallocHost(&ctx->pin, 2 * half));
+    for (cudaEvent_t &e : ctx->pin_ev) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const size_t nch = (bytes + half - 1) / half;
+  for (size_t c = 0; c < nch; ++c) {
+    char *pin = reinterpret_cast<char *>(ctx->pin) + (c & 1) * half;
+    if (c >= 2) CU(cudaEventSynchronize(ctx->pin_ev[c & 1]));  // this half's previous chunk is on the device
+    const size_t lo = c * half, len = std::min(half, bytes - lo);
+    const char *sp = static_cast<const char *>(src) + lo;
+    parallel_range((long long)len, [pin, sp](long long a, long long b) { memcpy(pin + a, sp + a, (size_t)(b - a)); });
+    CU(cudaMemcpyAsync(static_cast<char *>(dst) + lo, pin, len, cudaMemcpyHostToDevice, st));
+    CU(cudaEventRecord(ctx->pin_ev[c & 1], st));
+  }
+  for (size_t c = nch > 2 ? nch - 2 : 0; c < nch; ++c) CU(cudaEventSynchronize(ctx->pin_ev[c & 1]));
   return KWB_OK;
 }
 

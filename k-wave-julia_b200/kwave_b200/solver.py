@@ -57,12 +57,15 @@ def _findall(mask, shape) -> np.ndarray:
     if m.shape != tuple(shape):
         raise ValueError(f"mask of shape {m.shape} does not match the grid {tuple(shape)}")
     if m.ndim > 1 and 4 * int(np.count_nonzero(m)) <= m.size:
-        # sparse: coordinates in row-major order, then column-major linear index, sorted
-        coords = np.nonzero(m)
-        lin = np.zeros(coords[0].size, dtype=np.int64)
-        for ax in range(m.ndim - 1, -1, -1):
-            lin *= m.shape[ax]
-            lin += coords[ax]
+        # sparse: row-major flat indices of the points (one scan of the mask), mapped to
+        # column-major linear indices and sorted
+        k = np.flatnonzero(m.reshape(-1))
+        lin = np.zeros(k.size, dtype=np.int64)
+        col_stride = 1
+        for ax in range(m.ndim):
+            c, k = np.divmod(k, int(np.prod(m.shape[ax + 1:], dtype=np.int64)))
+            lin += c * col_stride
+            col_stride *= m.shape[ax]
         lin.sort()
         return lin
     return np.ascontiguousarray(np.flatnonzero(m.ravel(order="F")).astype(np.int64))
