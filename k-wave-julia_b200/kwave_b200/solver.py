@@ -139,8 +139,9 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
                   elastic: bool = False) -> _Built:
     """Normalise the reference's arguments into a kwb_problem (first_order.jl:311-441, 529-669).
 
-    ``elastic=True`` takes an ``ElasticMedium`` and ``ElasticSource`` for the stress-velocity
-    solver (solver/elastic.jl:133-588): p0 is not smoothed and time-reversal data is not used.
+    An ``ElasticMedium`` (or ``elastic=True``) selects the stress-velocity solver
+    (solver/elastic.jl:133-588) with an ``ElasticSource``: p0 is not smoothed and time-reversal
+    data is not used.
 
     ``extra_sensors`` (not in the reference API) adds further sensor groups -- (mask, record)
     pairs given as ``KWaveSensor`` or dicts -- so one solve can record different fields on
@@ -162,6 +163,7 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
     P.Nt = int(kgrid.Nt)
     P.row_major = 1  # grid arrays go over as NumPy (row-major) buffers; see _flat
     P.axisymmetric = 1 if axisymmetric else 0
+    elastic = elastic or isinstance(medium, ElasticMedium)
     P.elastic = 1 if elastic else 0
     if elastic and D not in (2, 3):
         raise TypeError("the elastic solver takes a 2D or 3D grid")
@@ -380,8 +382,7 @@ def _alloc_outputs(ctx: Context, b: _Built, kgrid: KWaveGrid):
     return O, outs, arrays, pfull
 
 
-def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt_loop: int,
-             post_filters: bool = True):
+def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt_loop: int):
     dicts = []
     for g, d in enumerate(arrays):
         data = {}
@@ -392,7 +393,7 @@ def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt
     extra = dicts[1:] if sensor.mask is not None else dicts
     if pfull is not None:
         main["p_final"] = pfull
-    if post_filters:  # the elastic solvers return the recorded data as it is
+    if not b.problem.elastic:  # the elastic solvers return the recorded data as it is
         apply_sensor_directivity(main, sensor, kgrid)
         apply_frequency_response(main, sensor, kgrid)
     out = SimulationOutput(main)
@@ -495,7 +496,7 @@ def _pstd_elastic(kgrid, medium, source, sensor, pml_size, pml_alpha, progress_c
     with ctx.lock:
         O, outs, arrays, pfull = _alloc_outputs(ctx, b, kgrid)
         check(ctx.lib, ctx.handle, ctx.lib.kwb_solve(ctx.handle, C.byref(b.problem), C.byref(O)))
-    return _collect(b, arrays, pfull, sensor, kgrid, int(b.problem.Nt), post_filters=False)
+    return _collect(b, arrays, pfull, sensor, kgrid, int(b.problem.Nt))
 
 
 def pstd_elastic_2d(kgrid: KWaveGrid, medium: ElasticMedium, source: ElasticSource, sensor: KWaveSensor,
@@ -527,10 +528,8 @@ class Simulation:
         self.ctx = context or default_context()
         self.kgrid, self.sensor = kgrid, sensor
         # an ElasticMedium selects the elastic solver (pstd_elastic_2d/3d)
-        self.elastic = isinstance(medium, ElasticMedium)
         self.b = build_problem(kgrid, medium, source, sensor, pml_size=pml_size,
-                               pml_alpha=pml_alpha, smooth_p0=smooth_p0, extra_sensors=extra_sensors,
-                               elastic=self.elastic)
+                               pml_alpha=pml_alpha, smooth_p0=smooth_p0, extra_sensors=extra_sensors)
         self.Nt = int(self.b.problem.tr.n_cols if self.b.problem.tr.data else self.b.problem.Nt)
         h = C.c_void_p()
         with self.ctx.lock:
@@ -565,7 +564,7 @@ class Simulation:
     def outputs(self) -> SimulationOutput:
         O, outs, arrays, pfull = _alloc_outputs(self.ctx, self.b, self.kgrid)
         self._chk(self.ctx.lib.kwb_sim_read_outputs(self.handle, C.byref(O)))
-        return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt, post_filters=not self.elastic)
+        return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt)
 
     def profile(self, steps: int) -> list:
         kt = _lib.KernelTimes()
@@ -677,7 +676,8 @@ def solve_prepared(prep: Prepared) -> SimulationOutput:
 
 def submit(kgrid, medium, source, sensor, *, pml_size=20, pml_alpha=2.0, smooth_p0=True,
            extra_sensors=(), context: Optional[Context] = None) -> Request:
-    """Queue one simulation for continuous batching; returns a Request (non-blocking)."""
+    """Queue one simulation for continuous batching; returns a Request (non-blocking).  An
+    ``ElasticMedium`` queues an elastic solve (the same scheduler serves both solvers)."""
     return submit_prepared(prepare(kgrid, medium, source, sensor, pml_size=pml_size, pml_alpha=pml_alpha,
                                    smooth_p0=smooth_p0, extra_sensors=extra_sensors, context=context))
 

@@ -258,3 +258,26 @@ def test_register_and_stockham_paths_agree(kb, monkeypatch):
     for path in outs:
         assert_parity(outs[path], ref, TOL_L2, TOL_MAX)
     assert_parity(outs["default"], outs["generic"], 1e-5, 1e-4)
+
+
+def test_served_with_fluid_requests(kb):
+    """Elastic and fluid requests served together by the continuous-batching scheduler give the
+    same outputs as their blocking solves."""
+    from kwave_b200.workloads import elastic3d, c4_sim
+    jobs = []
+    for n in (32, 48):
+        case = elastic3d(n, Nt=40)
+        g, m, s, sen, kw = case.to_api()
+        jobs.append((g, m, s, sen, kw, kb.pstd_elastic_3d))
+    for i in range(2):
+        case = c4_sim(i, sides=(128, 192), nt_range=(60, 90))
+        g, m, s, sen, kw = case.to_api()
+        jobs.append((g, m, s, sen, kw, kb.kspace_first_order))
+    reqs = [kb.submit(g, m, s, sen, **kw) for g, m, s, sen, kw, _ in jobs]
+    for (g, m, s, sen, kw, solve), r in zip(jobs, reqs):
+        served = r.result(timeout=120)
+        if solve is kb.pstd_elastic_3d:
+            kw = {k: v for k, v in kw.items() if k != "smooth_p0"}
+        direct = solve(g, m, s, sen, **kw)
+        for k in direct.keys():
+            assert np.array_equal(served[k], direct[k]), k
