@@ -776,12 +776,30 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   }
 
   // ---- tile shapes and FFT plans
+  CU(cudaDeviceGetAttribute(&h.num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
   for (int a = 0; a < 3; ++a) make_plan(h.N[a], h.plan[a]);
   h.L_line[0] = choose_L(h.N[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, 0, false);
   for (int a = 1; a < 3; ++a) h.L_line[a] = choose_L(h.N[a], 8, (h.N[0] + 1) / 2, 0, false);
   h.L_eosx = choose_L(h.N[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, h.dispersion, true);
   for (int a = 1; a < 3; ++a) h.L_spec[a] = choose_L(h.N[a], 8, h.n1, h.dispersion, true);
   h.L_spec[0] = 1;
+  {
+    // Small grids: fewer lines per tile until the shared-memory (Stockham) passes fill the GPU --
+    // a 384^2 grid otherwise runs its x pass as 39 CTAs and its y spectrum pass as 25.  Strided
+    // line passes stop at one wave and keep 4 complex lines (8 columns: one 32-byte sector per
+    // row), since narrower tiles waste most of each sector they read.
+    const long long NS = h.num_sms;
+    auto shrink = [&](int &L, long long want, int floor_L, auto tiles) {
+      while (L > floor_L && tiles(L) < want) L = std::max(floor_L, (L + 1) / 2);
+    };
+    const long long N0 = h.N[0], N1 = h.N[1], N2 = h.N[2];
+    shrink(h.L_line[0], 4 * NS, 1, [&](int L) { return (N1 + 2 * L - 1) / (2 * L) * N2; });
+    shrink(h.L_line[1], NS, 4, [&](int L) { return (N0 + 2 * L - 1) / (2 * L) * N2; });
+    shrink(h.L_line[2], NS, 4, [&](int L) { return (N0 + 2 * L - 1) / (2 * L) * N1; });
+    shrink(h.L_eosx, 4 * NS, 1, [&](int L) { return (N1 + 2 * L - 1) / (2 * L) * N2; });
+    shrink(h.L_spec[1], 4 * NS, 1, [&](int L) { return (h.n1 + L - 1) / L * N2; });
+    shrink(h.L_spec[2], 4 * NS, 1, [&](int L) { return (h.n1 + L - 1) / L * N1; });
+  }
 
   // ---- admission by free device memory
   {
@@ -1218,7 +1236,6 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
       break;
     }
   }
-  CU(cudaDeviceGetAttribute(&h.num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
   CU(h.elastic ? el_prime(h) : prime_attributes(h));
 
   // ---- device descriptor
