@@ -158,3 +158,55 @@ def test_post_filters_match_the_oracle_per_row():
     d = {"p": p.copy()}
     apply_sensor_directivity(d, sen, g)
     assert np.array_equal(d["p"][[0, 5, 9]], p[[0, 5, 9]])
+
+
+def test_build_problem_elastic():
+    """ElasticMedium/ElasticSource -> kwb_problem: speeds, density, Kelvin-Voigt coefficients only
+    where the 2D homogeneous branch uses them, stress signals per component, p0 unsmoothed, and
+    the reference's error cases."""
+    from kwave_b200.solver import build_problem
+    n = 16
+    g = kb.KWaveGrid(n, 1e-4, n, 1e-4)
+    g.dt, g.Nt = 1e-8, 12
+    p0 = np.zeros((n, n))
+    p0[5, 7] = 3.0
+    s_mask = np.zeros((n, n), bool)
+    s_mask[2, 3] = s_mask[9, 1] = True
+    sig = np.arange(2 * 12, dtype=float).reshape(2, 12)
+    src = kb.ElasticSource(s_mask=s_mask, sxx=sig, syy=2 * sig, szz=3 * sig, sxy=4 * sig, s_mode=kb.Dirichlet, p0=p0)
+    med = kb.ElasticMedium(3000.0, 1500.0, 1800.0, alpha_coeff_compression=0.5, alpha_coeff_shear=1.0,
+                           alpha_power=1.5)
+    sen = kb.KWaveSensor(mask=np.ones((n, n), bool), record=["p", "I_avg"])
+    P = build_problem(g, med, src, sen, data_cast=np.float32).problem  # I_avg allowed: no MethodError here
+    assert P.elastic == 1 and P.c0.count == 1 and P.cs.count == 1 and P.rho0.count == 1
+    assert P.cs.data[0] == 1500.0 and P.c0.data[0] == 3000.0 and P.rho0.data[0] == 1800.0
+    assert P.alpha_mode != 0 and P.alpha_coeff == 0.5 and P.has_alpha_shear == 1 and P.alpha_coeff_shear == 1.0
+    assert P.alpha_power == 1.5
+    assert P.n_s_index == 2 and [P.s_index[i] for i in range(2)] == [9 + 1 * n, 2 + 3 * n]  # sorted, column-major
+    assert P.s_mode == int(kb.Dirichlet)
+    # 2D reads sxx, syy, sxy only (elastic.jl:315-347)
+    assert [bool(P.s_signal[k].data) for k in range(6)] == [True, True, False, True, False, False]
+    assert P.s_signal[3].n_rows == 2 and P.s_signal[3].n_cols == 12
+    # p0 goes over unsmoothed (row-major buffer)
+    got = np.ctypeslib.as_array(P.p0.data, shape=(n * n,)).reshape(n, n)
+    assert np.array_equal(got, p0)
+    # heterogeneous density: chi unused, so no absorption fields
+    rho = np.full((n, n), 1800.0)
+    P2 = build_problem(g, kb.ElasticMedium(np.full((n, n), 3000.0), 1500.0, rho, alpha_coeff_compression=0.5,
+                                           alpha_power=1.5), kb.ElasticSource(p0=p0), sen).problem
+    assert P2.alpha_mode == 0 and P2.has_alpha_shear == 0 and P2.c0.count == n * n and P2.rho0.count == n * n
+    # 3D: no chi either
+    g3 = kb.KWaveGrid(8, 1e-4, 8, 1e-4, 8, 1e-4)
+    g3.dt, g3.Nt = 1e-8, 4
+    P3 = build_problem(g3, med, kb.ElasticSource(), kb.KWaveSensor(mask=np.ones((8, 8, 8), bool))).problem
+    assert P3.elastic == 1 and P3.alpha_mode == 0 and P3.has_alpha_shear == 0
+    # errors: scalar density with array speeds (a matrix power in the reference), 1D grids,
+    # stress signals with too few rows
+    with pytest.raises(TypeError):
+        build_problem(g, kb.ElasticMedium(np.full((n, n), 3000.0), 1500.0, 1800.0), kb.ElasticSource(), sen)
+    g1 = kb.KWaveGrid(32, 1e-4)
+    g1.dt, g1.Nt = 1e-8, 4
+    with pytest.raises(TypeError):
+        build_problem(g1, med, kb.ElasticSource(), kb.KWaveSensor(mask=np.ones(32, bool)))
+    with pytest.raises(IndexError):
+        build_problem(g, med, kb.ElasticSource(s_mask=s_mask, sxx=np.ones((1, 12))), sen)
