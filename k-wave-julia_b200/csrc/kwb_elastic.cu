@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   extern __shared__ float4 smem_raw[];
   const int N = S.N[axis];
   const int L = S.L_line[axis];
-  const int LS = N + 1;
+  const int LS = line_pitch(N);
   const int Nx = S.N[0];
   float2 *X = reinterpret_cast<float2 *>(smem_raw);
   float2 *Y = X + L * LS;

@@ -143,11 +143,21 @@ struct Dft<7, INV> {
   }
 };
 
-// One Stockham stage of radix R over L lines: X -> Y.
+// Line pitch (float2 slots per line) of the Stockham buffers: N elements plus one pad slot per 16
+// for the intermediate stages (see spad), plus one.
+__host__ __device__ inline int line_pitch(int N) { return N + (N >> 4) + 1; }
+
+// Slot of element m in an intermediate stage buffer: one pad slot after every 16 elements, so
+// the strided stores of the early stages (stride R * Ns with Ns < 16) fall in distinct banks.
+// The first stage reads, and the last stage writes, the natural (unpadded) order the callers
+// use.
+__device__ __forceinline__ int spad(int m) { return m + (m >> 4); }
+
+// One Stockham stage of radix R over L lines: X -> Y (pin / pout: X / Y in the padded layout).
 template <int R, bool INV>
 __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ X, float2 *__restrict__ Y,
                                                int L, int LS, int N, int Ns,
-                                               const float2 *__restrict__ tw) {
+                                               const float2 *__restrict__ tw, bool pin, bool pout) {
   const int NR = N / R;
   const int total = L * NR;
   const int tstride = N / (Ns * R);
@@ -159,7 +169,10 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ X, flo
     float2 *y = Y + l * LS;
     float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = x[j + r * NR];
+    for (int r = 0; r < R; ++r) {
+      const int m = j + r * NR;
+      v[r] = x[pin ? spad(m) : m];
+    }
     if (k != 0) {
       const int ts = k * tstride;
 #pragma unroll
@@ -172,11 +185,14 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ X, flo
     Dft<R, INV>::run(v);
     const int base = (j - k) * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) y[base + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) {
+      const int m = base + r * Ns;
+      y[pout ? spad(m) : m] = v[r];
+    }
   }
 }
 
-// Transform L lines held in X (Y is scratch of the same size).  Returns the buffer holding the
+// Transform L lines held in X (Y is scratch of the same size; line pitch LS >= line_pitch(N)).  Returns the buffer holding the
 // result (X or Y).  Caller must __syncthreads() before (X filled) -- this function syncs after
 // every stage, so the result is visible to all threads on return.
 template <bool INV>
@@ -186,13 +202,14 @@ __device__ float2 *fft_lines(float2 *X, float2 *Y, int L, int LS, const FftPlan 
   int Ns = 1;
   for (int s = 0; s < plan.nstages; ++s) {
     const int R = plan.radix[s];
+    const bool pin = s > 0, pout = s + 1 < plan.nstages;
     switch (R) {
-      case 2: stockham_stage<2, INV>(X, Y, L, LS, N, Ns, tw); break;
-      case 3: stockham_stage<3, INV>(X, Y, L, LS, N, Ns, tw); break;
-      case 4: stockham_stage<4, INV>(X, Y, L, LS, N, Ns, tw); break;
-      case 5: stockham_stage<5, INV>(X, Y, L, LS, N, Ns, tw); break;
-      case 7: stockham_stage<7, INV>(X, Y, L, LS, N, Ns, tw); break;
-      default: stockham_stage<8, INV>(X, Y, L, LS, N, Ns, tw); break;
+      case 2: stockham_stage<2, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
+      case 3: stockham_stage<3, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
+      case 4: stockham_stage<4, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
+      case 5: stockham_stage<5, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
+      case 7: stockham_stage<7, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
+      default: stockham_stage<8, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
     }
     __syncthreads();
     float2 *t = X;

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
 
   const int N = S.N[axis];
   const int L = S.L_line[axis];
-  const int LS = N + 1;
+  const int LS = line_pitch(N);
   const int Nx = S.N[0];
   float2 *X = smem;
   float2 *Y = X + L * LS;
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   if (t >= S.Nt) return;
   const int N = S.N[0];
   const int L = S.L_eosx;
-  const int LS = N + 1;
+  const int LS = line_pitch(N);
   const int two = S.dispersion;
   const int LL = two ? 2 * L : L;
   float2 *X = smem;
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   if (t >= S.Nt) return;
   const int N = S.N[0];
   const int L = S.L_eosx;
-  const int LS = N + 1;
+  const int LS = line_pitch(N);
   float2 *X = smem;
   float2 *Y = X + L * LS;
   float2 *tw = Y + L * LS;
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   if (t >= S.Nt) return;
   const int N = S.N[axis];
   const int L = S.L_spec[axis];
-  const int LS = N + 1;
+  const int LS = line_pitch(N);
   const int two = S.dispersion && op != KWB_SPEC_INV;
   const int LL = two ? 2 * L : L;
   float2 *X = smem;
@@ -521,9 +521,9 @@ __global__ void k_advance_t0(long long *t0, long long k) {
 // launchers
 // ------------------------------------------------------------------------------------------
 
-size_t line_pass_smem(int N, int L) { return ((size_t)2 * L * (N + 1) + N) * sizeof(float2); }
+size_t line_pass_smem(int N, int L) { return ((size_t)2 * L * line_pitch(N) + N) * sizeof(float2); }
 size_t spec_pass_smem(int N, int L, int dispersion) {
-  return ((size_t)2 * (dispersion ? 2 * L : L) * (N + 1) + N) * sizeof(float2);
+  return ((size_t)2 * (dispersion ? 2 * L : L) * line_pitch(N) + N) * sizeof(float2);
 }
 
 static int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
