@@ -16,6 +16,7 @@
 
 #define KWB_MAX_STAGES 16
 #define KWB_THREADS 256
+#define KWB_PASS_THREADS_MAX 1024  // Stockham passes on grids with few tiles (pass_threads)
 #define KWB_MAX_N 4096
 #define KWB_CHUNK_STEPS 32  // time steps per replayed CUDA graph
 
@@ -136,6 +137,7 @@ struct SimDev {
 
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
+  int grid_fill;      // Stockham passes of small grids: narrower tiles and larger CTAs to fill the GPU
 
   // Elastic solver (pstd_elastic_2d/3d).  u[d] are the velocities, p the recorded pressure
   // -trace(sigma)/D.  el_s: stresses in the slots xx, yy, zz, xy, xz, yz (2-D: 0, 1, 3).  el_w:
@@ -199,6 +201,7 @@ struct GroupDev {
 namespace kwb {
 size_t line_pass_smem(int N, int L);
 size_t spec_pass_smem(int N, int L, int dispersion);
+int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile);
 cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
                              long long step_s, cudaStream_t st);
 cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long step_s,

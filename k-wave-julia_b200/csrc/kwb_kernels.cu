@@ -28,7 +28,7 @@ namespace kwb {
 // ------------------------------------------------------------------------------------------
 
 template <bool CONTIG>
-__global__ void __launch_bounds__(KWB_THREADS)
+__global__ void __launch_bounds__(KWB_PASS_THREADS_MAX)
     k_line_pass(const SimDev *__restrict__ sims, int axis, int mode, long long step_s) {
   KWB_STEP_KERNEL_PROLOGUE();
   extern __shared__ float4 smem_raw[];
@@ -528,6 +528,16 @@ size_t spec_pass_smem(int N, int L, int dispersion) {
 
 static int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Threads per CTA of a Stockham line pass: KWB_THREADS, or up to KWB_PASS_THREADS_MAX when the
+// pass launches fewer than four CTAs per SM, so that a small grid's few tiles are not each worked
+// through by 256 threads in long serial loops (the EOS and spectrum passes, shorter per tile,
+// keep 256).
+int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile) {
+  if (!h.grid_fill || tiles >= 4LL * (h.num_sms > 0 ? h.num_sms : 148)) return KWB_THREADS;
+  const long long t = (elems_per_tile / 4 + 31) / 32 * 32;
+  return (int)std::min<long long>(KWB_PASS_THREADS_MAX, std::max<long long>(KWB_THREADS, t));
+}
+
 // The dynamic shared-memory limit of a kernel is a per-function attribute.  It is raised once to
 // the device's opt-in maximum, so simulations of different sizes in one process never lower
 // it under one another.
@@ -550,10 +560,11 @@ cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int
   int tiles;
   if (axis == 0) {
     tiles = cdiv(h.N[1], 2 * L) * h.N[2];
-    kwb_launch(k_line_pass<true>, tiles, KWB_THREADS, sm, st, d_sim, axis, mode, step_s);
+    kwb_launch(k_line_pass<true>, tiles, pass_threads(h, tiles, (long long)L * h.N[0]), sm, st, d_sim, axis, mode, step_s);
   } else {
     tiles = cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]);
-    kwb_launch(k_line_pass<false>, tiles, KWB_THREADS, sm, st, d_sim, axis, mode, step_s);
+    kwb_launch(k_line_pass<false>, tiles, pass_threads(h, tiles, (long long)L * h.N[axis]), sm, st, d_sim, axis, mode,
+               step_s);
   }
   return cudaGetLastError();
 }

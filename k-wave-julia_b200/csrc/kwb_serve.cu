@@ -31,6 +31,7 @@ cudaStream_t kwb_sim_stream_of(kwb_sim *S);
 long long kwb_sim_nt_of(const kwb_sim *S);
 void kwb_ctx_set_err(kwb_ctx *ctx, const char *msg);
 int kwb_ctx_device(const kwb_ctx *ctx);
+void kwb_ctx_set_batched(kwb_ctx *ctx);
 
 namespace {
 
@@ -266,6 +267,7 @@ static KwbServer *server_of(kwb_ctx *ctx, KwbServer *&slot) {
     KwbServer *s = new KwbServer();
     s->owner = ctx;
     kwb_context_create(kwb_ctx_device(ctx), &s->inner);
+    if (s->inner) kwb_ctx_set_batched(s->inner);
     s->th = std::thread([s] { s->loop(); });
     slot = s;
   }
