@@ -50,7 +50,7 @@ __device__ __forceinline__ Coord coord_of(const SimDev &S, long long i) {
 
 // Directional derivatives of g.nf fields along `axis` on one tile of 2L real lines.
 template <bool CONTIG>
-__global__ void __launch_bounds__(KWB_THREADS)
+__global__ void __launch_bounds__(KWB_PASS_THREADS_MAX)
     k_el_grad(const __grid_constant__ SimDev S, int axis, const __grid_constant__ ElGrad g, long long step_s) {
   extern __shared__ float4 smem_raw[];
   const int N = S.N[axis];
@@ -399,11 +399,13 @@ cudaError_t el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cud
   if (el_fast(h, axis)) return fast_el_grad(h, axis, g, s, st);
   const int L = h.L_line[axis];
   const size_t sm = line_pass_smem(h.N[axis], L);
+  const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * L) * h.N[2]
+                                    : (long long)cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]);
+  const int threads = pass_threads(h, tiles, (long long)L * h.N[axis]);
   if (axis == 0)
-    kwb_launch(k_el_grad<true>, cdiv(h.N[1], 2 * L) * h.N[2], KWB_THREADS, sm, st, h, axis, g, s);
+    kwb_launch(k_el_grad<true>, (int)tiles, threads, sm, st, h, axis, g, s);
   else
-    kwb_launch(k_el_grad<false>, cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]), KWB_THREADS, sm, st, h,
-               axis, g, s);
+    kwb_launch(k_el_grad<false>, (int)tiles, threads, sm, st, h, axis, g, s);
   return cudaGetLastError();
 }
 
