@@ -416,3 +416,21 @@ def test_fused_x_pass_and_eos_match_separate_kernels(kb, wl, monkeypatch):
         sep = run_gpu(case)
         assert np.array_equal(fused["p"], sep["p"]), plane
         assert np.array_equal(fused.extra[0]["p_max"], sep.extra[0]["p_max"]), plane
+
+
+def test_small_grid_tiles_do_not_change_results(kb, monkeypatch):
+    """The small-grid tile choice (narrower tiles and larger CTAs for a simulation that runs alone)
+    changes only how lines are distributed over CTAs: fields are bit-identical with it off."""
+    from kwave_b200.workloads import c2, elastic3d
+    outs = {}
+    for fill in ("1", "0"):
+        monkeypatch.setenv("KWB_GRID_FILL", fill)
+        case = c2(n=270, Nt=60)
+        g, m, s, sen, kw = case.to_api()
+        fluid = kb.kspace_first_order(g, m, s, sen, **kw)
+        ecase = elastic3d(48, Nt=30)
+        eg, em, es, esen, ekw = ecase.to_api()
+        outs[fill] = (fluid, kb.pstd_elastic_3d(eg, em, es, esen, **ekw))
+    for a, b in zip(outs["1"], outs["0"]):
+        for k in b.keys():
+            assert np.array_equal(a[k], b[k]), k
