@@ -450,3 +450,40 @@ def test_elastic_s_wave_matches_leapfrog_recurrence():
         u_ref[:, t] = np.real(np.fft.ifft(V))
     assert np.allclose(r["uy"], u_ref, rtol=0, atol=1e-12)
     assert np.abs(r["p"]).max() < 1e-12
+
+
+def test_elastic_kelvin_voigt_factor_in_2d_homogeneous_branch():
+    """With alpha_coeff_compression set, the 2D homogeneous stress update scales the constitutive
+    term by (1 + chi_p) (solver/elastic.jl:282-295): the plane P wave follows the leapfrog recurrence
+    with (lambda + 2 mu)(1 + chi_p) and lambda (1 + chi_p)."""
+    n, dx, steps = 32, 0.5e-3, 40
+    g = K.KWaveGrid(n, dx, n, dx)
+    g.dt, g.Nt = 5e-8, steps
+    x = np.arange(n)
+    line = np.cos(2 * math.pi * 4 * x / n)
+    p0 = np.repeat(line[:, None], n, axis=1)
+    mask = np.zeros((n, n), bool)
+    mask[:, 2] = True
+    rho, cp, cs = 1800.0, 3000.0, 1500.0
+    med = K.ElasticMedium(cp, cs, rho, alpha_coeff_compression=0.8, alpha_coeff_shear=0.3, alpha_power=1.3)
+    chi_p, _ = K.elastic_chi(med)
+    assert chi_p > 0
+    r = K.pstd_elastic_2d(g, med, K.ElasticSource(p0=p0), K.KWaveSensor(mask=mask, record=["p"]), pml_size=0)
+    lam, mu = rho * (cp ** 2 - 2 * cs ** 2), rho * cs ** 2
+    _, gp, gn = _plane_wave_modes(n, dx, 0)
+    S = -np.fft.fft(line)
+    T = S.copy()
+    V = np.zeros(n, complex)
+    p_ref = np.zeros((n, steps))
+    for t in range(steps):
+        V = V + g.dt / rho * gp * S
+        S, T = (S + g.dt * (1 + chi_p) * (lam + 2 * mu) * gn * V, T + g.dt * (1 + chi_p) * lam * gn * V)
+        p_ref[:, t] = np.real(np.fft.ifft(-(S + T) / 2))
+    assert np.allclose(r["p"], p_ref, rtol=0, atol=1e-12 * np.abs(p_ref).max())
+    # a heterogeneous density takes the branch without chi
+    r2 = K.pstd_elastic_2d(g, K.ElasticMedium(cp, cs, np.full((n, n), rho), alpha_coeff_compression=0.8,
+                                              alpha_power=1.3),
+                           K.ElasticSource(p0=p0), K.KWaveSensor(mask=mask, record=["p"]), pml_size=0)
+    r0 = K.pstd_elastic_2d(g, K.ElasticMedium(cp, cs, rho), K.ElasticSource(p0=p0),
+                           K.KWaveSensor(mask=mask, record=["p"]), pml_size=0)
+    assert np.allclose(r2["p"], r0["p"], rtol=0, atol=1e-12 * np.abs(r0["p"]).max())
