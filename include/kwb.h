@@ -10,7 +10,10 @@
  *                                                 287-306, 505-524; sensor.jl:76-82)
  *
  * A Julia shim (ccall) or any other host builds one kwb_problem from those four structs and
- * the keyword arguments and calls kwb_solve().  Everything here is plain C: host pointers,
+ * the keyword arguments and calls kwb_solve().  The same problem struct also carries the
+ * axisymmetric solver (kspace_first_order_as, solver/axisymmetric.jl:26-227; the axisymmetric
+ * flag) and the elastic solvers (pstd_elastic_2d / pstd_elastic_3d, solver/elastic.jl:133-588;
+ * the elastic flag and fields).  Everything here is plain C: host pointers,
  * 64-bit sizes, FP64 inputs and outputs, negative status codes instead of exceptions.
  *
  * Array convention: every grid-shaped input is FP64 in the reference's column-major order

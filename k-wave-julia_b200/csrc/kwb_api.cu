@@ -3,7 +3,8 @@
 //
 // The set-up restates the allocation and pre-computation half of kspace_first_order
 // (KWave.jl/src/solver/first_order.jl:92-441 for 1D/2D, 505-669 for 3D); the stepping restates
-// its time loop (first_order.jl:232-266, 448-484, 677-713) with the kernels of kwb_kernels.cu.
+// its time loop (first_order.jl:232-266, 448-484, 677-713) with the kernels of kwb_fast.cu and
+// kwb_kernels.cu; elastic problems step through elastic_step (kernels in kwb_elastic.cu).
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>

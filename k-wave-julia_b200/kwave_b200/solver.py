@@ -6,6 +6,11 @@ exactly where the reference does, smooth p0 on the host in FP64 (first_order_ste
 109-111, 157-159), build one ``kwb_problem`` and call ``kwb_solve``; then apply the reference's
 post-loop host filters (first_order_steps.jl:836-910) and return a ``SimulationOutput``.
 
+``kspace_first_order_as`` (solver/axisymmetric.jl:26-227) and ``pstd_elastic_2d`` /
+``pstd_elastic_3d`` (solver/elastic.jl:133-588) go through the same ``kwb_problem`` with its
+axisymmetric or elastic fields set; the elastic solvers return the recorded data without the
+post-loop filters, as the reference does.
+
 Errors the reference raises are raised here with the same meaning: an unset time array, an
 invalid record field, signals with too few rows (BoundsError), ``:I_avg``/``:I_max`` with
 ``data_cast=Float32`` (MethodError in ``_acoustic_intensity``), array ``alpha_coeff``.
