@@ -7,7 +7,8 @@ source and sensor, then call ``kspace_first_order``.  The time loop runs in libk
 
 from .core import (Additive, AdditiveNoCorrection, Dirichlet, ElasticMedium, ElasticSource, KWaveGrid, KWaveMedium, KWaveSensor,
                    KWaveSource, SimulationOutput, SourceMode, VALID_RECORD_FIELDS, db2neper,
-                   get_optimal_pml_size, get_pml, make_ball, make_circle, make_disc, make_line,
+                   get_optimal_pml_size, get_pml, grid_size, grid_spacing, k_max, make_ball, make_circle,
+                   make_disc, make_line, total_grid_points,
                    make_time, neper2db, smooth, tone_burst, validate_record_fields)
 from ._lib import KWaveB200Error, LIB_PATH, load_library
 from .solver import (Context, Prepared, Request, Simulation, prepare, solve_prepared, submit_prepared, build_problem, default_context, estimate_device_bytes,
@@ -24,4 +25,5 @@ __all__ = [
     "default_context", "kspace_first_order", "kspace_first_order_as", "Request", "estimate_device_bytes", "serving_config",
     "serving_stats", "shard_jobs", "solve_batch", "submit", "Prepared", "prepare", "solve_prepared",
     "submit_prepared", "ElasticMedium", "ElasticSource", "pstd_elastic_2d", "pstd_elastic_3d",
+    "grid_size", "grid_spacing", "k_max", "total_grid_points",
 ]

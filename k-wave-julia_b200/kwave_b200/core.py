@@ -6,7 +6,8 @@ returns them.  Everything here runs once per simulation on the host in FP64 (the
 it on the host too); the time stepping itself is on the GPU (``solver.py``).
 
 Mirrors:
-  KWaveGrid / make_time               KWave.jl/src/grid.jl:120-352
+  KWaveGrid / make_time, grid_size,   KWave.jl/src/grid.jl:120-352
+  grid_spacing, k_max, total_grid_points
   KWaveMedium                         KWave.jl/src/medium.jl:248-341
   KWaveSource, SourceMode             KWave.jl/src/source.jl:160-230, types.jl:355
   ElasticMedium, ElasticSource        KWave.jl/src/solver/elastic.jl:22-104
@@ -86,6 +87,26 @@ class KWaveGrid:
 
     def total_grid_points(self) -> int:
         return int(np.prod(self.N))
+
+
+def total_grid_points(grid: KWaveGrid) -> int:
+    """grid.jl:260-262."""
+    return grid.total_grid_points()
+
+
+def grid_size(grid: KWaveGrid) -> tuple:
+    """grid.jl:269-271: (Nx[, Ny[, Nz]])."""
+    return tuple(grid.N)
+
+
+def grid_spacing(grid: KWaveGrid) -> tuple:
+    """grid.jl:278-280: (dx[, dy[, dz]])."""
+    return tuple(grid.d)
+
+
+def k_max(grid: KWaveGrid) -> float:
+    """grid.jl:294-296: the Nyquist wavenumber pi / max spacing [rad/m]."""
+    return min(math.pi / d for d in grid.d)
 
 
 def make_time(grid: KWaveGrid, sound_speed, cfl: float = 0.3, t_end: Optional[float] = None):

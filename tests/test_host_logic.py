@@ -210,3 +210,11 @@ def test_build_problem_elastic():
         build_problem(g1, med, kb.ElasticSource(), kb.KWaveSensor(mask=np.ones(32, bool)))
     with pytest.raises(IndexError):
         build_problem(g, med, kb.ElasticSource(s_mask=s_mask, sxx=np.ones((1, 12))), sen)
+
+
+def test_grid_helpers():  # grid.jl:260-296
+    g = kb.KWaveGrid(64, 1e-4, 32, 2e-4, 16, 5e-5)
+    assert kb.grid_size(g) == (64, 32, 16) and kb.grid_spacing(g) == (1e-4, 2e-4, 5e-5)
+    assert kb.total_grid_points(g) == 64 * 32 * 16
+    assert kb.k_max(g) == min(math.pi / 1e-4, math.pi / 2e-4, math.pi / 5e-5)
+    assert kb.k_max(kb.KWaveGrid(10, 1e-3)) == math.pi / 1e-3
