@@ -487,3 +487,46 @@ def test_elastic_kelvin_voigt_factor_in_2d_homogeneous_branch():
     r0 = K.pstd_elastic_2d(g, K.ElasticMedium(cp, cs, rho), K.ElasticSource(p0=p0),
                            K.KWaveSensor(mask=mask, record=["p"]), pml_size=0)
     assert np.allclose(r2["p"], r0["p"], rtol=0, atol=1e-12 * np.abs(r0["p"]).max())
+
+
+@pytest.mark.parametrize("j,d", [(0, 1), (0, 2), (1, 0), (1, 2), (2, 0), (2, 1)])
+def test_elastic_3d_shear_waves_match_leapfrog_recurrence(j, d):
+    """3D: a kick in velocity component j that varies along axis d (j != d) is a plane shear wave
+    through the stress slot {j, d}: per mode, v_j <- v_j + dt/rho G+_d s_jd, s_jd <- s_jd + dt mu
+    G-_d v_j; p stays 0 and the other velocity components stay 0."""
+    n, dx, steps = 16, 0.5e-3, 30
+    g = K.KWaveGrid(n, dx, n, dx, n, dx)
+    g.dt, g.Nt = 5e-8, steps
+    line = np.cos(2 * math.pi * 3 * np.arange(n) / n)
+    shape = [1, 1, 1]
+    shape[d] = n
+    field = np.broadcast_to(line.reshape(shape), (n, n, n))
+    kick = np.zeros((n ** 3, steps))
+    kick[:, 0] = field.ravel(order="F")  # column-major points of the full mask
+    comps = {"ux": None, "uy": None, "uz": None}
+    comps["u" + "xyz"[j]] = kick
+    mask = np.zeros((n, n, n), bool)
+    idx = [4, 5, 6]
+    idx[d] = slice(None)
+    mask[tuple(idx)] = True
+    rec = ["p", "ux", "uy", "uz"]
+    rho, cp, cs = 1800.0, 3000.0, 1500.0
+    r = K.pstd_elastic_3d(g, K.ElasticMedium(cp, cs, rho),
+                          K.ElasticSource(u_mask=np.ones((n, n, n), bool), **comps),
+                          K.KWaveSensor(mask=mask, record=rec), pml_size=0)
+    mu = rho * cs ** 2
+    _, gp, gn = _plane_wave_modes(n, dx, 0)
+    V = np.zeros(n, complex)
+    Sh = np.zeros(n, complex)
+    u_ref = np.zeros((n, steps))
+    for t in range(steps):
+        V = V + g.dt / rho * gp * Sh
+        if t == 0:
+            V = V + np.fft.fft(line)
+        Sh = Sh + g.dt * mu * gn * V
+        u_ref[:, t] = np.real(np.fft.ifft(V))
+    assert np.allclose(r["u" + "xyz"[j]], u_ref, rtol=0, atol=1e-12)
+    for k in range(3):
+        if k != j:
+            assert np.abs(r["u" + "xyz"[k]]).max() < 1e-12
+    assert np.abs(r["p"]).max() < 1e-9 * mu * dx
