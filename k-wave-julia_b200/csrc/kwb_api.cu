@@ -130,6 +130,11 @@ double pairwise_sum(const double *x, long long n) {
   return pairwise_sum(x, h) + pairwise_sum(x + h, n - h);
 }
 
+}  // namespace
+
+namespace kwb {
+
+// Stockham stage radices of a line of N points: 8s first, then 4 or 2, then 3, 5, 7.
 bool make_plan(int N, FftPlan &pl) {
   pl.n = N;
   pl.nstages = 0;
@@ -163,6 +168,10 @@ int choose_L(int N, int want, int cap_lines, int dispersion, bool spec) {
   if (L < 1) L = 1;
   return L;
 }
+
+}  // namespace kwb
+
+namespace {
 
 // Stream-ordered device scratch for simulation set-up (FP64 staging of the medium): freed on
 // the set-up stream when the creating call returns, so it holds no memory afterwards.

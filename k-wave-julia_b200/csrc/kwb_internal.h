@@ -199,6 +199,11 @@ struct GroupDev {
 
 // Kernel launchers (kwb_kernels.cu).
 namespace kwb {
+// Stockham plan of a line of N points (false: a prime factor above 7 or too many stages), and
+// the complex lines per tile of a line pass (spec = false) or spectrum pass (spec = true) that
+// fit the shared-memory budget, at most cap_lines (kwb_api.cu).
+bool make_plan(int N, FftPlan &pl);
+int choose_L(int N, int want, int cap_lines, int dispersion, bool spec);
 size_t line_pass_smem(int N, int L);
 size_t spec_pass_smem(int N, int L, int dispersion);
 int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile);

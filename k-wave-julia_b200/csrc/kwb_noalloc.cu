@@ -46,41 +46,20 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 std::mutex g_mu;
 void *g_base[KWB_NOALLOC_MAX_DEVICES];
-std::string g_err;
+// Last error of this host thread: concurrent callers (one per device, say) never share it.
+thread_local std::string g_err;
 
 int fail(int code, const char *msg) {
   g_err = msg;
   return code;
 }
 
-bool plan_of(int N, FftPlan &pl) {
-  pl.n = N;
-  pl.nstages = 0;
-  int n = N;
-  int a = 0;
-  while (n % 2 == 0) {
-    n /= 2;
-    ++a;
-  }
-  while (a >= 3) {
-    pl.radix[pl.nstages++] = 8;
-    a -= 3;
-  }
-  if (a == 2) pl.radix[pl.nstages++] = 4;
-  if (a == 1) pl.radix[pl.nstages++] = 2;
-  for (int p : {3, 5, 7})
-    while (n % p == 0 && pl.nstages < KWB_MAX_STAGES) {
-      pl.radix[pl.nstages++] = p;
-      n /= p;
-    }
-  return n == 1;
-}
-
-int lines_for(int N, int want, int cap, bool spec) {
-  int L = want < 1 ? 1 : want;
-  while (L > 1 && (spec ? kwb::spec_pass_smem(N, L, 0) : kwb::line_pass_smem(N, L)) > 200 * 1024) L /= 2;
-  if (cap > 0 && L > cap) L = cap;
-  return L < 1 ? 1 : L;
+// Writes the kernel descriptor into the scratch array and zeroes the device step base.  The
+// descriptor travels as a kernel parameter (copied when the launch is issued), so no host
+// buffer has to outlive the call.
+__global__ void k_noalloc_setup(const __grid_constant__ SimDev h, SimDev *dst, long long *t0) {
+  *dst = h;
+  *t0 = 0;
 }
 
 // Device address of the scratch array on `device`; looked up once per device with that device
@@ -115,13 +94,22 @@ extern "C" int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t 
   if (ndim < 1 || ndim > 3 || !N_in || !d_in || !rho || !p) return fail(KWB_E_INVALID, "bad arguments");
   if (alpha_mode == KWB_STOKES && !c0sq)
     return fail(KWB_E_UNSUPPORTED, "the dispersion branch (scalar c0 with :stokes) is not offered without allocation");
-  if (!(dt > 0) || !(c_ref > 0)) return fail(KWB_E_INVALID, "dt and c_ref must be positive");
+  if (!(dt > 0) || !(c_ref > 0) || !std::isfinite(dt) || !std::isfinite(c_ref))
+    return fail(KWB_E_INVALID, "dt and c_ref must be finite and positive");
+  if (alpha_mode != KWB_NO_ABSORPTION && alpha_mode != KWB_NO_DISPERSION && alpha_mode != KWB_STOKES)
+    return fail(KWB_E_INVALID, "alpha_mode must be KWB_NO_ABSORPTION, KWB_NO_DISPERSION or KWB_STOKES");
+  if (alpha_mode != KWB_NO_ABSORPTION && (!std::isfinite(alpha_coeff) || !std::isfinite(alpha_power)))
+    return fail(KWB_E_INVALID, "alpha_coeff and alpha_power must be finite");
+  if (!c0sq && !(std::isfinite(c0sq_scalar) && c0sq_scalar > 0))
+    return fail(KWB_E_INVALID, "c0sq_scalar must be finite and positive when c0sq is NULL");
+  if (nonlinear && !nlq && !std::isfinite(nlq_scalar))
+    return fail(KWB_E_INVALID, "nlq_scalar must be finite when nlq is NULL");
   SimDev h{};
   h.ndim = h.D = ndim;
   for (int a = 0; a < 3; ++a) {
     const int64_t n = a < ndim ? N_in[a] : 1;
     if (n < 1 || n > KWB_MAX_N) return fail(KWB_E_UNSUPPORTED, "grid side outside 1..4096");
-    if (!plan_of((int)n, h.plan[a])) return fail(KWB_E_UNSUPPORTED, "grid side has a prime factor above 7");
+    if (!make_plan((int)n, h.plan[a])) return fail(KWB_E_UNSUPPORTED, "grid side has a prime factor above 7");
     h.N[a] = (int)n;
     if (a < ndim && !rho[a]) return fail(KWB_E_INVALID, "rho component pointer is NULL");
   }
@@ -163,8 +151,8 @@ extern "C" int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t 
   for (int a = 0; a < 3; ++a) h.tw[a] = reinterpret_cast<float2 *>(base + kOffTw + (size_t)a * KWB_MAX_N * 8);
   h.L_line[0] = 1;
   h.L_line[1] = h.L_line[2] = 1;
-  h.L_eosx = lines_for(h.N[0], 2048 / h.N[0], (h.N[1] + 1) / 2, true);
-  for (int a = 1; a < 3; ++a) h.L_spec[a] = lines_for(h.N[a], 8, h.n1, true);
+  h.L_eosx = choose_L(h.N[0], 2048 / h.N[0], (h.N[1] + 1) / 2, 0, true);
+  for (int a = 1; a < 3; ++a) h.L_spec[a] = choose_L(h.N[a], 8, h.n1, 0, true);
   h.Nt = 1;
   h.t0 = reinterpret_cast<long long *>(base + kOffT0);
 
@@ -181,8 +169,11 @@ extern "C" int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t 
 
   cudaError_t e = prime_attributes(h);
   // The step base must start at zero; every other region is fully rewritten below.
-  if (e == cudaSuccess) e = cudaMemsetAsync(base + kOffT0, 0, sizeof(long long), st);
-  if (e == cudaSuccess) e = cudaMemcpyToSymbolAsync(g_noalloc_scratch, &h, sizeof(h), kOffSim, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    k_noalloc_setup<<<1, 1, 0, st>>>(h, reinterpret_cast<SimDev *>(base + kOffSim),
+                                     reinterpret_cast<long long *>(base + kOffT0));
+    e = cudaGetLastError();
+  }
   for (int a = 0; a < ndim && e == cudaSuccess; ++a) e = build_twiddles(const_cast<float2 *>(h.tw[a]), h.N[a], st);
   if (e == cudaSuccess)
     e = build_eos_multiplier(const_cast<float *>(h.M), nullptr, h.N, d3, c_ref, dt, csq_fold, absorbing, tau, 0.0, y, nullptr, st);

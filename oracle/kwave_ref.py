@@ -54,7 +54,8 @@ from typing import Any, Optional, Sequence
 import numpy as np
 import scipy.fft as sfft
 
-_WORKERS = os.cpu_count() or 1
+# scipy.fft worker threads: all host cores unless KWB_ORACLE_WORKERS says otherwise
+_WORKERS = int(os.environ.get("KWB_ORACLE_WORKERS", "0")) or os.cpu_count() or 1
 
 DIRICHLET, ADDITIVE, ADDITIVE_NO_CORRECTION = 0, 1, 2  # types.jl:11 (@enum SourceMode)
 
