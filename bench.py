@@ -38,6 +38,73 @@ UNIT = "Gvoxel-steps/s"
 METRIC = "Gvoxel-steps/s (fluid k-space time stepping)"
 
 
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def rel_errors(gpu, ref):
+    """(relative L2, max abs error / max |ref|) of a result against the FP64 oracle's."""
+    import numpy as np
+    a = np.asarray(gpu, dtype=np.float64).ravel()
+    b = np.asarray(ref, dtype=np.float64).ravel()
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b) / nb), float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def c3_accuracy(case, out):
+    """Errors of a full 256^3 x 1500-step solve against the FP64 oracle's run of all 1500 steps
+    (tests/golden/c3_long.npz): the plane p series at its 1024 sampled points and the volume p_max
+    at every 4th voxel along each axis."""
+    import numpy as np
+    path = os.path.join(GOLDEN, "c3_long.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "no full-horizon FP64 golden for this workload"}
+    gold = np.load(path)
+    plane_rows = np.flatnonzero(np.asarray(case.sensor["mask"]).ravel(order="F"))
+    rows = np.searchsorted(plane_rows, gold["plane_idx"])
+    l2p, mxp = rel_errors(out["p"][rows, :], gold["p"])
+    l2v, mxv = rel_errors(out.extra[0]["p_max"][gold["vol_idx"]], gold["p_max"])
+    return {"reference": "FP64 oracle, all 1500 steps (tests/golden/c3_long.npz)",
+            "p": {"rel_l2": l2p, "max_rel": mxp, "sample": f"{len(rows)} plane points x {gold['p'].shape[1]} steps"},
+            "p_max": {"rel_l2": l2v, "max_rel": mxv, "sample": f"{len(gold['vol_idx'])} voxels (every 4th per axis)"}}
+
+
+def c2_leg(ctx, warmup=40):
+    """The 512^2 x 2000-step heterogeneous absorbing solve: every step device-timed in one
+    advance (CUDA events), and its full-grid p_max / p_rms against the FP64 oracle's 2000-step
+    run (tests/golden/c2_long.npz)."""
+    import numpy as np
+    import kwave_b200 as kb
+    from kwave_b200 import workloads
+    warm = workloads.c2(Nt=warmup)
+    g, m, s, sen, kw = warm.to_api()
+    w = kb.Simulation(g, m, s, sen, context=ctx, **kw)
+    w.advance_timed(warmup)
+    w.close()
+    case = workloads.c2()
+    g, m, s, sen, kw = case.to_api()
+    sim = kb.Simulation(g, m, s, sen, context=ctx, **kw)
+    ms = sim.advance_timed(case.Nt)
+    out = sim.outputs()
+    sched = sim.schedule()
+    sim.close()
+    peak, kind = peaks()
+    value = case.voxels * case.Nt / (ms / 1e3) / 1e9
+    res = {"workload": case.name, "grid": list(case.N), "steps": case.Nt, "ms_per_step": ms / case.Nt,
+           "value": value, "unit": UNIT,
+           "spm": {"bytes_per_voxel_step": 4.0 * SPM_WORDS["c2"],
+                   "frac": 4.0 * SPM_WORDS["c2"] * value / peak, "peak_kind": f"{kind} copy bandwidth"},
+           "schedule": sched}
+    path = os.path.join(GOLDEN, "c2_long.npz")
+    if os.path.exists(path):
+        gold = np.load(path)
+        acc = {"reference": "FP64 oracle, all 2000 steps (tests/golden/c2_long.npz)"}
+        for k in ("p_max", "p_rms"):
+            l2, mx = rel_errors(out[k], gold[k])
+            acc[k] = {"rel_l2": l2, "max_rel": mx}
+        res["accuracy"] = acc
+    return res
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -391,10 +458,19 @@ def serving_bench(ctx, n_req=48, rate=200.0, seed=5005, nt_range=(300, 800), max
     t_end = max(t0 + arrivals[i] + lat[i] for i in range(n_req))
     span = t_end - t0
     q = lambda a, x: float(np.percentile(np.asarray(a), x))
+    accuracy = None
+    gpath = os.path.join(GOLDEN, "serving_sample.npz")
+    if os.path.exists(gpath) and (seed, nt_range, n_req) == (5005, (300, 800), 48):
+        gold = np.load(gpath)
+        accuracy = {"reference": "FP64 oracle (tests/golden/serving_sample.npz)"}
+        for i in gold["requests"]:
+            l2, mx = rel_errors(reqs[int(i)][1].result()["p"], gold[f"p_{int(i)}"])
+            accuracy[cases[int(i)].name] = {"rel_l2": l2, "max_rel": mx}
     res = {"workload": f"{n_req} Poisson requests at {rate:.0f}/s, 70% 2D 256-1024 / 30% 3D 64^3-192^3, "
                        f"Nt {nt_range[0]}-{nt_range[1]}",
            "max_running": max_running,
-           "sims_per_s": n_req / span, "p50_latency_s": q(lat, 50), "p99_latency_s": q(lat, 99)}
+           "sims_per_s": n_req / span, "p50_latency_s": q(lat, 50), "p99_latency_s": q(lat, 99),
+           "accuracy_sampled": accuracy}
     if not one_at_a_time:
         return res
     preps1 = prep_all()
@@ -424,6 +500,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the Poisson serving measurement")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT-based comparator")
     ap.add_argument("--no-elastic", action="store_true", help="skip the elastic-solver measurement")
+    ap.add_argument("--no-c2", action="store_true", help="skip the 512^2 x 2000-step solve")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
@@ -482,7 +559,11 @@ def main():
         e2e = {"value": world * vox * case.Nt / el / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d / case.Nt), "d2h_bytes_per_step": int(d2h / case.Nt),
                "solve_s": el, "steps": case.Nt}
+        accuracy = c3_accuracy(case, out) if args.config == "c3" else None
+    else:
+        accuracy = None
 
+    c2 = None if (args.no_c2 or args.config == "c2") else c2_leg(ctx)
     batch = None if args.no_batch else batch_bench(ctx)
     serve = None if args.no_serve else serving_bench(ctx)
 
@@ -519,6 +600,8 @@ def main():
                     "frac": spm_frac},
             "kernels": kernels,
             "e2e": e2e,
+            "accuracy": accuracy,
+            "c2": c2,
             "batch": batch,
             "serving": serve,
             "cpu_baseline": cpu,

@@ -85,6 +85,22 @@ typedef struct kwb_sensor_group {
   uint8_t record_count[KWB_REC_COUNT]; /* times each field appears in sensor.record; the running
                             sums of p_rms, u_rms and I_avg are added that many times per step
                             (record_sensor_data! loops over the record list) */
+  /* Post-loop filters of this group's pressure series, the reference's
+   * apply_sensor_directivity! and apply_frequency_response! (first_order_steps.jl:836-910),
+   * applied on the device before read-back (fluid solvers; the elastic solvers have none).
+   * Each replaces p_j by real(ifft(fft(p_j) .* H)) along time, directivity first:
+   *   directivity_angle != NULL: H = sinc(2 pi |f| / d_min * directivity_size * sin(theta_j) / 2),
+   *     theta_j = directivity_angle[0] for every point (n_directivity_angle == 1) or
+   *     directivity_angle[j] (n_directivity_angle >= the number of points); points whose angle
+   *     is exactly 0 are not filtered by it; d_min = dx (1-D) or the smallest grid spacing;
+   *   has_frequency_response != 0: H = exp(-(|f| - frequency_center)^2 / (2 frequency_bandwidth^2)).
+   * f = fftfreq(Nt, 1/dt).  Only the "p" series is filtered, as in the reference. */
+  const double *directivity_angle;
+  int64_t n_directivity_angle;
+  double directivity_size;
+  int32_t has_frequency_response;
+  double frequency_center;
+  double frequency_bandwidth;
 } kwb_sensor_group;
 
 /* Optional per-step callback, the reference's progress_callback(t_index, Nt, p)
@@ -218,6 +234,14 @@ typedef struct kwb_kernel_times {
   double bytes_per_launch[16];  /* algorithmic bytes one launch moves (operand reads + writes) */
 } kwb_kernel_times;
 int kwb_sim_profile(kwb_sim *sim, int64_t steps, kwb_kernel_times *out);
+
+/* The FFT schedule the simulation's time step runs with, as text: where it came from ("tuned"
+ * on first use of the grid shape, "cache" from an earlier measurement of it, or "heuristic"
+ * when tuning is off), then the per-pass choices.  Measured schedules play the role of the
+ * reference's FFTW.MEASURE plans (fft_utils.jl:59-60); they are cached per device and shape in
+ * memory and in the file KWB_TUNE_CACHE (default $HOME/.cache/kwb/fft_schedules.txt; "none"
+ * keeps no file).  KWB_TUNE=0 keeps the size heuristic. */
+int kwb_sim_schedule(const kwb_sim *sim, char *buf, int64_t len);
 
 /* Device bytes the simulation holds and kernels launched per time step. */
 int kwb_sim_info(const kwb_sim *sim, int64_t *device_bytes, int32_t *launches_per_step);

@@ -11,10 +11,14 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "../../include/kwb.h"
 #include "kwb_internal.h"
@@ -135,7 +139,7 @@ double pairwise_sum(const double *x, long long n) {
 namespace kwb {
 
 // Stockham stage radices of a line of N points: 8s first, then 4 or 2, then 3, 5, 7.
-bool make_plan(int N, FftPlan &pl) {
+bool make_plan_order(int N, FftPlan &pl, int order) {
   pl.n = N;
   pl.nstages = 0;
   int n = N, a = 0;
@@ -143,21 +147,36 @@ bool make_plan(int N, FftPlan &pl) {
     n /= 2;
     ++a;
   }
-  while (a >= 3) {
-    pl.radix[pl.nstages++] = 8;
-    a -= 3;
-  }
-  if (a == 2) pl.radix[pl.nstages++] = 4;
-  if (a == 1) pl.radix[pl.nstages++] = 2;
+  int odd[KWB_MAX_STAGES], nodd = 0;
   for (int p : {3, 5, 7}) {
     while (n % p == 0) {
-      if (pl.nstages >= KWB_MAX_STAGES) return false;
-      pl.radix[pl.nstages++] = p;
+      if (nodd >= KWB_MAX_STAGES) return false;
+      odd[nodd++] = p;
       n /= p;
     }
   }
-  return n == 1;
+  if (n != 1) return false;
+  auto push = [&](int r) {
+    if (pl.nstages >= KWB_MAX_STAGES) return false;
+    pl.radix[pl.nstages++] = r;
+    return true;
+  };
+  if (order == 2)
+    for (int i = 0; i < nodd; ++i)
+      if (!push(odd[i])) return false;
+  const int big = order == 1 ? 2 : 3;  // log2 of the largest power-of-two radix
+  while (a >= big)
+    if (!push(1 << big)) return false;
+    else a -= big;
+  if (a == 2 && !push(4)) return false;
+  if (a == 1 && !push(2)) return false;
+  if (order != 2)
+    for (int i = 0; i < nodd; ++i)
+      if (!push(odd[i])) return false;
+  return true;
 }
+
+bool make_plan(int N, FftPlan &pl) { return make_plan_order(N, pl, 0); }
 
 int choose_L(int N, int want, int cap_lines, int dispersion, bool spec) {
   int L = want;
@@ -240,6 +259,10 @@ struct GroupHost {
   GroupDev *d_dev = nullptr;
   long long n = 0;
   bool fused = false;  // updated inside the x C2R pass
+  // post-loop filters of the p series: distinct filters (sin(theta) of their directivity, NaN
+  // for none) and the filter of each point; empty when the group has no filter
+  std::vector<double> filt_sin;
+  std::vector<int> filt_of;
 };
 
 struct kwb_sim {
@@ -253,6 +276,9 @@ struct kwb_sim {
   long long Nt_loop = 0;
   long long Nt_grid = 0;
   long long steps_done = 0;
+  double d[3] = {1.0, 1.0, 1.0};  // grid spacing and time step (post-loop filters)
+  double dt = 0.0;
+  std::string schedule_src = "heuristic";  // where the FFT schedule came from (kwb_sim_schedule)
   std::vector<GroupHost> groups;
   bool tr = false;
   kwb_progress_fn progress = nullptr;
@@ -706,6 +732,120 @@ static int build_chunk_graph(kwb_sim *S) {
   return KWB_OK;
 }
 
+// ---- FFT schedule cache: key (device, library version, shape and the flags that select the
+// kernels) -> Schedule text; in memory for the process and, unless KWB_TUNE_CACHE=none, in a text
+// file (KWB_TUNE_CACHE, default $HOME/.cache/kwb/fft_schedules.txt), one "key<TAB>schedule" line each.
+static std::mutex g_sched_mu;
+static std::map<std::string, std::string> g_sched;
+static bool g_sched_loaded = false;
+
+static std::string sched_file() {
+  const char *e = getenv("KWB_TUNE_CACHE");
+  if (e && *e) return strcmp(e, "none") == 0 ? std::string() : std::string(e);
+  const char *home = getenv("HOME");
+  return home && *home ? std::string(home) + "/.cache/kwb/fft_schedules.txt" : std::string();
+}
+
+static void sched_load_locked() {
+  if (g_sched_loaded) return;
+  g_sched_loaded = true;
+  const std::string path = sched_file();
+  if (path.empty()) return;
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return;
+  char line[1024];
+  while (fgets(line, sizeof(line), f)) {
+    char *tab = strchr(line, '\t');
+    if (!tab) continue;
+    *tab = 0;
+    char *v = tab + 1;
+    v[strcspn(v, "\r\n")] = 0;
+    Schedule sc;
+    if (schedule_parse(v, sc)) g_sched[line] = v;  // later lines win
+  }
+  fclose(f);
+}
+
+static void sched_store_locked(const std::string &key, const std::string &val) {
+  g_sched[key] = val;
+  const std::string path = sched_file();
+  if (path.empty()) return;
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos && slash > 0) {  // create the directory chain
+    for (size_t i = 1; i <= slash; ++i)
+      if (path[i] == '/' || i == slash) mkdir(path.substr(0, i == slash ? slash : i).c_str(), 0755);
+  }
+  FILE *f = fopen(path.c_str(), "a");
+  if (!f) return;  // an unwritable cache only costs a re-measurement in the next process
+  fprintf(f, "%s\t%s\n", key.c_str(), val.c_str());
+  fclose(f);
+}
+
+static std::string sched_key(int device, const SimDev &h) {
+  cudaDeviceProp prop;
+  char name[256] = "unknown";
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) snprintf(name, sizeof(name), "%s/%d", prop.name, prop.multiProcessorCount);
+  char buf[512];
+  const char *eo = getenv("KWB_TUNE_ORDER");
+  snprintf(buf, sizeof(buf), "%.200s|v%d|nd%d|N%dx%dx%d|fast%d|plane%d|fuse%d|disp%d|fill%d|axi%d|rho%d|c%d|nl%d|ord%d",
+           name, KWB_VERSION, h.ndim, h.N[0], h.N[1], h.N[2], h.fast, h.plane, h.fuse_xeos, h.dispersion,
+           h.grid_fill, h.inv_r ? 1 : 0, h.rho0 ? 1 : 0, h.c0sq ? 1 : 0, (h.nonlinear && h.nlq) ? 2 : h.nonlinear,
+           (eo && strcmp(eo, "1") == 0) ? 1 : 0);
+  return buf;
+}
+
+// Pick the FFT schedule of a new simulation: KWB_TILE or KWB_TUNE=0 keep the size heuristic;
+// otherwise a cached measurement of this shape, or a new one (FFTW.MEASURE's role,
+// fft_utils.jl:59-60).  KWB_TUNE_PICK=i takes candidate i of every pass instead of measuring
+// (tests).  Measuring runs the passes on the simulation's buffers, so its state fields are
+// cleared afterwards.
+static int choose_schedule(kwb_sim *S, SimDev &h, cudaStream_t st) {
+  kwb_ctx *ctx = S->ctx;
+  const char *tn = getenv("KWB_TUNE");
+  const char *pk = getenv("KWB_TUNE_PICK");
+  if (h.tile_override >= 0 || (tn && strcmp(tn, "0") == 0)) return KWB_OK;
+  const int pick = pk && *pk ? atoi(pk) : -1;
+  const std::string key = sched_key(ctx->device, h);
+  Schedule sc;
+  if (pick < 0) {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    sched_load_locked();
+    auto it = g_sched.find(key);
+    if (it != g_sched.end() && schedule_parse(it->second.c_str(), sc)) {
+      schedule_apply(h, sc);
+      S->schedule_src = "cache";
+      return KWB_OK;
+    }
+  }
+  TempBuf tmp(st, ctx->pool);
+  SimDev *d_t;
+  CU(tmp.alloc(&d_t, 1));
+  std::string log;
+  const char *eo = getenv("KWB_TUNE_ORDER");
+  CU(tune_schedule(h, d_t, st, pick, eo && strcmp(eo, "1") == 0, &log));
+  CU(cudaStreamSynchronize(st));
+  // the measured passes wrote the state fields: back to the zero state
+  const long long nvox = h.nvox;
+  CU(cudaMemsetAsync(h.p, 0, nvox * 4, st));
+  for (int a = 0; a < h.D; ++a) {
+    CU(cudaMemsetAsync(h.u[a], 0, nvox * 4, st));
+    CU(cudaMemsetAsync(h.rho[a], 0, nvox * 4, st));
+  }
+  if (h.spec) CU(cudaMemsetAsync(h.spec, 0, h.nspec * sizeof(float2), st));
+  if (h.spec2) CU(cudaMemsetAsync(h.spec2, 0, h.nspec * sizeof(float2), st));
+  if (h.rho_prev) CU(cudaMemsetAsync(h.rho_prev, 0, nvox * 4, st));
+  schedule_of(h, sc);
+  if (pick >= 0) {
+    S->schedule_src = "pick " + std::to_string(pick);
+    return KWB_OK;
+  }
+  S->schedule_src = "tuned";
+  if (getenv("KWB_TUNE_LOG")) fprintf(stderr, "kwb tune %s: %s-> %s\n", key.c_str(), log.c_str(), schedule_str(sc).c_str());
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  sched_store_locked(key, schedule_str(sc));
+  return KWB_OK;
+}
+
 int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   if (!ctx || !out) return KWB_E_INVALID;
   *out = nullptr;
@@ -743,6 +883,8 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   const long long nvox = h.nvox;
   S->tr = P->tr.data != nullptr;
   S->Nt_grid = P->Nt;
+  for (int a = 0; a < 3; ++a) S->d[a] = a < P->ndim ? P->d[a] : 1.0;
+  S->dt = P->dt;
   S->Nt_loop = S->tr ? P->tr.n_cols : P->Nt;
   h.Nt = S->Nt_loop;
   h.elastic = P->elastic ? 1 : 0;
@@ -782,6 +924,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (fp && strcmp(fp, "eos") == 0) h.fast = 2;
     const char *tv = getenv("KWB_TILE");
     h.tile_override = -1;
+    memset(h.tile_var, -1, sizeof(h.tile_var));  // per-pass choices: the heuristic until tuned
     if (tv && strcmp(tv, "big") == 0) h.tile_override = 0;
     if (tv && strcmp(tv, "mid") == 0) h.tile_override = 1;
     if (tv && strcmp(tv, "small") == 0) h.tile_override = 2;
@@ -1017,9 +1160,9 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (h.dispersion) CU(M.alloc(&M2, h.nspec));
     int *slot_ky = nullptr;
     if (h.plane) {
-      std::vector<int> ky(h.N[1]);
-      fast_plane_slot_ky(h.N[1], ky.data());
-      CU(M.alloc(&slot_ky, h.N[1]));
+      std::vector<int> ky(h.N[1] + h.N[2]);
+      fast_plane_slots(h.N[1], h.N[2], ky.data());
+      CU(M.alloc(&slot_ky, ky.size()));
       if ((rc = upload(ctx, slot_ky, ky.data(), ky.size() * sizeof(int), st))) return rc;
     }
     const double d3[3] = {P->d[0], D > 1 ? P->d[1] : 1.0, D > 2 ? P->d[2] : 1.0};
@@ -1151,9 +1294,26 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     GroupHost &G = S->groups[g];
     G.spec = P->groups[g];
     G.spec.index = nullptr;
+    G.spec.directivity_angle = nullptr;  // copied below: the caller's array may not outlive the call
     if (G.spec.cartesian) continue;
     const kwb_sensor_group &in = P->groups[g];
     G.n = in.dense ? nvox : in.n_index;
+    if (!h.elastic && (in.record_mask & (1u << KWB_REC_P)) && G.n > 0 &&
+        (in.directivity_angle || in.has_frequency_response)) {
+      // one filter per distinct directivity angle (angle 0: no directivity for that point)
+      std::map<double, int> ids;
+      G.filt_of.resize(G.n);
+      for (long long j = 0; j < G.n; ++j) {
+        double th = 0.0;
+        if (in.directivity_angle) th = in.directivity_angle[in.n_directivity_angle == 1 ? 0 : j];
+        auto it = ids.find(th);
+        if (it == ids.end()) {
+          it = ids.emplace(th, (int)G.filt_sin.size()).first;
+          G.filt_sin.push_back(th == 0.0 ? NAN : std::sin(th));
+        }
+        G.filt_of[j] = it->second;
+      }
+    }
     GroupDev &gd = G.dev;
     gd.n = G.n;
     gd.dense = in.dense;
@@ -1258,6 +1418,13 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   }
   CU(h.elastic ? el_prime(h) : prime_attributes(h));
 
+  // ---- FFT schedule: measured on first use of this shape (simulations of the batching
+  // scheduler share the GPU with others, so they keep the heuristic)
+  if (!h.elastic && !ctx->batched && S->Nt_loop > 0) {
+    if ((rc = choose_schedule(S.get(), h, st))) return rc;
+    CU(prime_attributes(h));
+  }
+
   // ---- device descriptor
   CU(M.alloc(&S->d_sim, 1));
   if ((rc = upload(ctx, S->d_sim, &h, sizeof(SimDev), st))) return rc;
@@ -1359,6 +1526,39 @@ int kwb_sim_read_pressure(kwb_sim *S, float *p_host) {
   return KWB_OK;
 }
 
+// The reference's post-loop filters (first_order_steps.jl:836-910) on the device series of
+// group G, in place, before it is read back.  Applied once: the filters are cleared after.
+static int apply_post_filters(kwb_sim *S, GroupHost &G) {
+  kwb_ctx *ctx = S->ctx;
+  cudaStream_t st = S->stream;
+  const int Nt = (int)G.dev.nt_alloc;
+  const int nf = (int)G.filt_sin.size();
+  const long long n = G.n;
+  const SimDev &h = S->h;
+  double dmin = h.ndim == 1 ? S->d[0] : std::min(S->d[0], S->d[1]);
+  if (h.ndim == 3) dmin = std::min(dmin, S->d[2]);
+  TempBuf tmp(st, ctx->pool);
+  float *hk, *out;
+  double *H, *cosT, *sinv;
+  int *fid;
+  CU(tmp.alloc(&hk, (size_t)nf * Nt));
+  CU(tmp.alloc(&H, (size_t)nf * Nt));
+  CU(tmp.alloc(&cosT, Nt));
+  CU(tmp.alloc(&sinv, nf));
+  CU(tmp.alloc(&fid, n));
+  CU(tmp.alloc(&out, (size_t)n * Nt));
+  CU(cudaMemcpyAsync(sinv, G.filt_sin.data(), nf * sizeof(double), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(fid, G.filt_of.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+  CU(filter_build_kernels(hk, H, cosT, Nt, nf, sinv, G.spec.directivity_size, dmin, S->dt, G.spec.has_frequency_response,
+                          G.spec.frequency_center, G.spec.frequency_bandwidth, st));
+  CU(filter_apply(out, G.dev.ser_p, hk, fid, Nt, n, st));
+  CU(cudaMemcpyAsync(G.dev.ser_p, out, (size_t)n * Nt * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  CU(cudaStreamSynchronize(st));  // the host vectors above are read by the copies
+  G.filt_sin.clear();
+  G.filt_of.clear();
+  return KWB_OK;
+}
+
 int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
   if (!S || !out) return KWB_E_INVALID;
   kwb_ctx *ctx = S->ctx;
@@ -1400,6 +1600,7 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
       });
     };
     int rc;
+    if (want(KWB_REC_P) && !G.filt_sin.empty() && (rc = apply_post_filters(S, S->groups[g]))) return rc;
     if (want(KWB_REC_P) && (rc = get32(gd.ser_p, n * gd.nt_alloc, o.field[KWB_REC_P]))) return rc;
     for (int d = 0; d < 3; ++d)
       if (want(KWB_REC_UX + d) && (rc = get32(gd.ser_u[d], n * gd.nt_alloc, o.field[KWB_REC_UX + d]))) return rc;
@@ -1434,6 +1635,14 @@ void kwb_sim_destroy(kwb_sim *S) {
 }
 
 }  // extern "C"
+
+extern "C" int kwb_sim_schedule(const kwb_sim *S, char *buf, int64_t len) {
+  if (!S || !buf || len <= 0) return KWB_E_INVALID;
+  Schedule sc;
+  schedule_of(S->h, sc);
+  snprintf(buf, (size_t)len, "%s: %s", S->schedule_src.c_str(), schedule_str(sc).c_str());
+  return KWB_OK;
+}
 
 // accessors for the serving scheduler (kwb_serve.cu)
 cudaStream_t kwb_sim_stream_of(kwb_sim *S) { return S->stream; }

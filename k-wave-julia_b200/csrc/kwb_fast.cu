@@ -827,24 +827,20 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
   for (int idx = 0; idx < E; ++idx) v[idx] = xs[F::nat_of(tt, idx)];
   // dense pressure sensor (record_sensor_data!, first_order_steps.jl:732-752): prefetch the
-  // running max/min before the transform, update all fields as p is written
+  // running max (or, without one, the running min) before the transform, update all fields as p
+  // is written.  One prefetched field keeps the kernel within its register budget.
   const GroupDev *gd = S.dense_p;
   const unsigned gm = gd ? gd->mask : 0u;
   constexpr bool PFS = E <= 16;  // prefetch only while it fits in registers
-  float2 pm[PFS ? E : 1], pn[PFS ? E : 1];
+  float2 pm[PFS ? E : 1];
+  const bool pf_max = PFS && (gm & (1u << 1)), pf_min = PFS && !pf_max && (gm & (1u << 2));
   const long long ra = base + (long long)(2 * l) * N, rb = ra + N;
-  if (PFS && (gm & (1u << 1))) {
+  if (pf_max || pf_min) {
+    const float *pa = pf_max ? gd->pmax : gd->pmin;
 #pragma unroll
     for (int r = 0; r < E; ++r) {
       const int i = tt + G * r;
-      pm[PFS ? r : 0] = make_float2(va ? gd->pmax[ra + i] : 0.f, vb ? gd->pmax[rb + i] : 0.f);
-    }
-  }
-  if (PFS && (gm & (1u << 2))) {
-#pragma unroll
-    for (int r = 0; r < E; ++r) {
-      const int i = tt + G * r;
-      pn[PFS ? r : 0] = make_float2(va ? gd->pmin[ra + i] : 0.f, vb ? gd->pmin[rb + i] : 0.f);
+      pm[PFS ? r : 0] = make_float2(va ? pa[ra + i] : 0.f, vb ? pa[rb + i] : 0.f);
     }
   }
   F::sync();
@@ -865,8 +861,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const int i = tt + G * r;
-        if (va) a[i] = fmaxf(PFS ? pm[PFS ? r : 0].x : a[i], v[r].x);
-        if (vb) a[N + i] = fmaxf(PFS ? pm[PFS ? r : 0].y : a[N + i], v[r].y);
+        if (va) a[i] = fmaxf(pf_max ? pm[PFS ? r : 0].x : a[i], v[r].x);
+        if (vb) a[N + i] = fmaxf(pf_max ? pm[PFS ? r : 0].y : a[N + i], v[r].y);
       }
     }
     if (gm & (1u << 2)) {
@@ -874,8 +870,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
       for (int r = 0; r < E; ++r) {
         const int i = tt + G * r;
-        if (va) a[i] = fminf(PFS ? pn[PFS ? r : 0].x : a[i], v[r].x);
-        if (vb) a[N + i] = fminf(PFS ? pn[PFS ? r : 0].y : a[N + i], v[r].y);
+        if (va) a[i] = fminf(pf_min ? pm[PFS ? r : 0].x : a[i], v[r].x);
+        if (vb) a[N + i] = fminf(pf_min ? pm[PFS ? r : 0].y : a[N + i], v[r].y);
       }
     }
     if (gm & (1u << 3)) {
@@ -1026,111 +1022,106 @@ __device__ __forceinline__ unsigned cluster_rank() {
 
 // Plane pass: the spectrum is [z][kx][y] (k_eos_fwd_fast<PLANE>), so plane kx is NZ rows of NY
 // contiguous values.  The CL CTAs of a cluster share plane kx: CTA r holds z rows
-// [r RZ, (r+1) RZ) in shared memory and
-//   1. transforms its rows along y (contiguous lines, one warp per line) and keeps each row in
-//      register order: slot s = t + G idx holds k_y = FY::k_of(t, idx);
-//   2. after a cluster barrier, transforms along z the slots [r CY, (r+1) CY) of every row of
-//      the plane (lines spread over the warps as in the strided line passes, so that a warp's
-//      loads cover consecutive slots of one row), loading element z of a slot from the CTA that
-//      holds row z (distributed shared memory), multiplies by M[kx][k_z][slot] and transforms
-//      back, storing each element to the CTA it came from;
-//   3. after a second barrier, transforms its rows back along y and writes them to the plane.
+// [r RZ, (r+1) RZ) in shared memory.  Every line is transformed by one warp (exchanges need only
+// __syncwarp; the CTA never takes a block-wide barrier):
+//   1. each warp copies its rows in (cp.async), transforms them along y and stores each row back
+//      in register order (slot s = t + G idx holds k_y = F::k_of(t, idx)), XOR-swizzled:
+//      element c of row r sits at r NY + (c ^ (r & 15));
+//   2. after a cluster barrier, each warp transforms along z the slots [r CY, (r+1) CY) of the
+//      plane: lane t loads element z = t + G q from row t of CTA q (distributed shared memory;
+//      the swizzle puts the 16 rows a half-warp reads in distinct banks), multiplies by
+//      M[kx][slot][t E + idx] (two 16-byte loads per lane) and transforms back, storing each
+//      element to the CTA it came from;
+//   3. after a second barrier, each warp transforms its rows back along y and writes them to the
+//      plane.
 // The spectrum crosses HBM once in and once out per step, with the multiplier read once.
-template <class FY, class FZ, int CL>
+template <class F, int CL>
 __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 2)
     k_plane_fast(const __grid_constant__ SimDev S, long long step_s) {
-  constexpr int NY = FY::N, NZ = FZ::N, RZ = NZ / CL, CY = NY / CL;
-  constexpr int LY = KWB_PLANE_THREADS / FY::G, LZ = KWB_PLANE_THREADS / FZ::G;
-  static_assert(RZ == 2 * LY && CY % LZ == 0 && RZ == FZ::G, "plane tiling");
-  constexpr int XS = (LY * FY::LP > LZ * FZ::LP) ? LY * FY::LP : LZ * FZ::LP;
+  constexpr int NN = F::N, RZ = NN / CL, CY = NN / CL, E = F::E;
+  constexpr int W = KWB_PLANE_THREADS / 32;
+  static_assert(F::G == 32 && F::WARP_SYNC, "one warp per line");
+  static_assert(RZ == F::G, "element z = lane + G q must sit in row `lane` of CTA q");
+  static_assert(RZ % W == 0 && CY % W == 0 && E == 8, "plane tiling");
+  constexpr int RW = RZ / W, SW = CY / W;  // rows and z lines per warp
   extern __shared__ float4 smem_raw[];
-  float2 *data = reinterpret_cast<float2 *>(smem_raw);  // [RZ][NY]
-  float2 *xsb = data + RZ * NY;
-  float2 *twy = xsb + XS;
-  float2 *twz = twy + FY::TW;
+  float2 *data = reinterpret_cast<float2 *>(smem_raw);  // [RZ][NN], swizzled after step 1
+  float2 *xsb = data + RZ * NN;
+  float2 *tw = xsb + W * F::LP;
   // the twiddles are written once at set-up: built before waiting on the previous kernel
-  FY::build_tw(twy, S.tw[1]);
-  FZ::build_tw(twz, S.tw[2]);
+  // (Ny == Nz: one table serves both axes)
+  F::build_tw(tw, S.tw[1]);
   KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (t >= S.Nt) return;  // uniform over the cluster
+  __syncthreads();        // the twiddle table is complete
   const unsigned rank = cluster_rank();
   const int kx = blockIdx.x / CL;
-  const int tid = threadIdx.x;
-  const long long rstride = (long long)S.n1 * NY;  // between consecutive z rows of the plane
-  float2 *plane = S.spec + (long long)rank * RZ * rstride + (long long)kx * NY;
-  // rows in two groups, so that the first transforms start while the second group lands
-  constexpr int CPR = NY / 2;  // 16-byte chunks per row
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long rstride = (long long)S.n1 * NN;  // between consecutive z rows of the plane
+  float2 *plane = S.spec + (long long)rank * RZ * rstride + (long long)kx * NN;
+  float2 *xs = xsb + w * F::LP;
+  auto sw = [](int r, int c) { return r * NN + (c ^ (r & 15)); };
+
+  // 1. forward along y: the warp's rows are copied in one commit group each
 #pragma unroll
-  for (int g = 0; g < 2; ++g) {
-    for (int q = tid; q < LY * CPR; q += KWB_PLANE_THREADS) {
-      const int r = g * LY + q / CPR, c = q % CPR;
-      cp_async16(data + r * NY + 2 * c, plane + r * rstride + 2 * c, 16);
-    }
+  for (int i = 0; i < RW; ++i) {
+    const int r = w * RW + i;
+#pragma unroll
+    for (int c = lane; c < NN / 2; c += 32) cp_async16(data + r * NN + 2 * c, plane + r * rstride + 2 * c, 16);
     cp_async_commit();
   }
-
-  // 1. forward along y
-  {
-    const int tt = tid % FY::G, l = tid / FY::G;
-    float2 *xs = xsb + l * FY::LP;
 #pragma unroll
-    for (int g = 0; g < 2; ++g) {
-      if (g == 0) cp_async_wait<1>();
-      else cp_async_wait<0>();
-      __syncthreads();
-      float2 *row = data + (g * LY + l) * NY;
-      float2 v[FY::E];
+  for (int i = 0; i < RW; ++i) {
+    const int r = w * RW + i;
+    if (i == 0) cp_async_wait<RW - 1>();
+    else cp_async_wait<0>();
+    __syncwarp();
+    float2 v[E];
 #pragma unroll
-      for (int r = 0; r < FY::E; ++r) v[r] = row[tt + FY::G * r];
-      FY::fwd(v, xs, twy, tt);
+    for (int q = 0; q < E; ++q) v[q] = data[r * NN + lane + 32 * q];
+    __syncwarp();  // the row is read before any lane overwrites it swizzled
+    F::fwd(v, xs, tw, lane);
 #pragma unroll
-      for (int idx = 0; idx < FY::E; ++idx) row[tt + FY::G * idx] = v[idx];
-    }
+    for (int idx = 0; idx < E; ++idx) data[sw(r, lane + 32 * idx)] = v[idx];
   }
   cluster_barrier();
 
   // 2. along z, multiply, back along z
   {
-    const int l = tid % LZ, tt = tid / LZ;
-    float2 *xs = xsb + l * FZ::LP;
-    const float *__restrict__ Mp = S.M + (long long)kx * NZ * NY;
+    const float *__restrict__ Mp = S.M + (long long)kx * NN * NN;
+    const unsigned a_row = cta_smem_addr(data + lane * NN);
 #pragma unroll 1
-    for (int c0 = 0; c0 < CY; c0 += LZ) {
-      const int sl = (int)rank * CY + c0 + l;  // slot (register-order k_y) of this line
-      float m[FZ::E];
+    for (int i = 0; i < SW; ++i) {
+      const int sl = (int)rank * CY + w * SW + i;  // slot (register-order k_y) of this line
+      const unsigned a0 = a_row + (unsigned)((sl ^ (lane & 15)) * sizeof(float2));
+      float2 v[E];
 #pragma unroll
-      for (int idx = 0; idx < FZ::E; ++idx) m[idx] = __ldg(Mp + (long long)FZ::k_of(tt, idx) * NY + sl);
-      // element z = tt + G r is row tt of CTA r (RZ == G)
-      const unsigned a0 = cta_smem_addr(data + tt * NY + sl);
-      float2 v[FZ::E];
+      for (int q = 0; q < E; ++q) v[q] = cluster_ld(cluster_map(a0, (unsigned)q));
+      const float4 *mq = reinterpret_cast<const float4 *>(Mp + (long long)sl * NN + lane * E);
+      const float4 m0 = __ldg(mq), m1 = __ldg(mq + 1);
+      F::fwd(v, xs, tw, lane);
+      const float m[E] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
 #pragma unroll
-      for (int r = 0; r < FZ::E; ++r) v[r] = cluster_ld(cluster_map(a0, (unsigned)r));
-      FZ::fwd(v, xs, twz, tt);
+      for (int idx = 0; idx < E; ++idx) v[idx] = pmul(v[idx], pair(m[idx]));
+      F::inv(v, xs, tw, lane);
 #pragma unroll
-      for (int idx = 0; idx < FZ::E; ++idx) v[idx] = make_float2(v[idx].x * m[idx], v[idx].y * m[idx]);
-      FZ::inv(v, xs, twz, tt);
-#pragma unroll
-      for (int r = 0; r < FZ::E; ++r) cluster_st(cluster_map(a0, (unsigned)r), v[r]);
+      for (int q = 0; q < E; ++q) cluster_st(cluster_map(a0, (unsigned)q), v[q]);
     }
   }
   cluster_barrier();
 
   // 3. back along y, straight to the plane
-  {
-    const int tt = tid % FY::G, l = tid / FY::G;
-    float2 *xs = xsb + l * FY::LP;
 #pragma unroll 1
-    for (int g = 0; g < 2; ++g) {
-      const float2 *row = data + (g * LY + l) * NY;
-      float2 v[FY::E];
+  for (int i = 0; i < RW; ++i) {
+    const int r = w * RW + i;
+    float2 v[E];
 #pragma unroll
-      for (int idx = 0; idx < FY::E; ++idx) v[idx] = row[tt + FY::G * idx];
-      FY::inv(v, xs, twy, tt);
-      float2 *out = plane + (g * LY + l) * rstride;
+    for (int idx = 0; idx < E; ++idx) v[idx] = data[sw(r, lane + 32 * idx)];
+    F::inv(v, xs, tw, lane);
+    float2 *out = plane + r * rstride;
 #pragma unroll
-      for (int r = 0; r < FY::E; ++r) out[tt + FY::G * r] = v[r];
-    }
+    for (int q = 0; q < E; ++q) out[lane + 32 * q] = v[q];
   }
 }
 
@@ -1164,8 +1155,9 @@ static bool want_small(const SimDev &h, long long tiles_big) {
 }
 
 // Tile variant per pass: 0 = big (THREADS per CTA), 1 = mid (128 threads), 2 = small (one warp).
-static int tile_variant(const SimDev &h, long long tiles_big) {
+static int tile_variant(const SimDev &h, int slot, long long tiles_big) {
   if (h.tile_override >= 0) return h.tile_override;
+  if (slot >= 0 && h.tile_var[slot] >= 0) return h.tile_var[slot];
   return want_small(h, tiles_big) ? 2 : 0;
 }
 
@@ -1257,7 +1249,7 @@ static cudaError_t launch_line_n(const SimDev *d_sim, const SimDev &h, int axis,
   constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
   const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * BIG) * h.N[2]
                                     : (long long)cdiv(h.N[0], 2 * BIG) * (axis == 1 ? h.N[2] : h.N[1]);
-  switch (tile_variant(h, tiles)) {
+  switch (tile_variant(h, KWB_SLOT_LINE0 + axis, tiles)) {
     case 1: line_go<N, MID>(d_sim, h, axis, mode, s, st); break;
     case 2: line_go<N, SMALL>(d_sim, h, axis, mode, s, st); break;
     default: line_go<N, BIG>(d_sim, h, axis, mode, s, st); break;
@@ -1314,7 +1306,7 @@ static cudaError_t launch_eos_n(const SimDev *d_sim, const SimDev &h, bool fwd, 
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
   constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
-  switch (tile_variant(h, (long long)cdiv(h.N[1], 2 * BIG) * h.N[2])) {
+  switch (tile_variant(h, fwd ? KWB_SLOT_EOS_FWD : KWB_SLOT_EOS_INV, (long long)cdiv(h.N[1], 2 * BIG) * h.N[2])) {
     case 1: eos_go<N, MID>(d_sim, h, fwd, s, st); break;
     case 2: eos_go<N, SMALL>(d_sim, h, fwd, s, st); break;
     default: eos_go<N, BIG>(d_sim, h, fwd, s, st); break;
@@ -1337,7 +1329,7 @@ static cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, int axis,
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
   constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
-  switch (tile_variant(h, (long long)cdiv(h.n1, BIG) * (axis == 1 ? h.N[2] : h.N[1]))) {
+  switch (tile_variant(h, KWB_SLOT_SPEC1 + axis - 1, (long long)cdiv(h.n1, BIG) * (axis == 1 ? h.N[2] : h.N[1]))) {
     case 1: spec_go<N, MID>(d_sim, h, axis, op, s, st); break;
     case 2: spec_go<N, SMALL>(d_sim, h, axis, op, s, st); break;
     default: spec_go<N, BIG>(d_sim, h, axis, op, s, st); break;
@@ -1346,16 +1338,13 @@ static cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, int axis,
 }
 
 // Cluster plane pass for Ny = Nz = 256: 8 CTAs of 512 threads per kx plane, 32 rows each.
-using PlaneFY = LinePolicy<256>::F<true>;
-using PlaneFZ = LinePolicy<256>::F<false>;
+using PlaneF = LinePolicy<256>::F<true>;
 constexpr int kPlaneCL = 8;
 constexpr size_t plane_smem() {
-  constexpr int RZ = 256 / kPlaneCL, LY = KWB_PLANE_THREADS / PlaneFY::G, LZ = KWB_PLANE_THREADS / PlaneFZ::G;
-  constexpr int XS = (LY * PlaneFY::LP > LZ * PlaneFZ::LP) ? LY * PlaneFY::LP : LZ * PlaneFZ::LP;
-  return ((size_t)RZ * 256 + XS + PlaneFY::TW + PlaneFZ::TW) * sizeof(float2);
+  return ((size_t)256 / kPlaneCL * 256 + (KWB_PLANE_THREADS / 32) * PlaneF::LP + PlaneF::TW) * sizeof(float2);
 }
 static int plane_clusters_per_device() {
-  const void *fn = (const void *)k_plane_fast<PlaneFY, PlaneFZ, kPlaneCL>;
+  const void *fn = (const void *)k_plane_fast<PlaneF, kPlaneCL>;
   if (raise_smem(fn, plane_smem()) != cudaSuccess) return 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(kPlaneCL * 16);
@@ -1529,7 +1518,7 @@ static cudaError_t launch_el_n(const SimDev &h, int axis, const ElGrad &g, long 
   constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
   const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * BIG) * h.N[2]
                                     : (long long)cdiv(h.N[0], 2 * BIG) * (axis == 1 ? h.N[2] : h.N[1]);
-  switch (tile_variant(h, tiles)) {
+  switch (tile_variant(h, KWB_SLOT_LINE0 + axis, tiles)) {
     case 1: el_go<N, MID>(h, axis, g, s, st); break;
     case 2: el_go<N, SMALL>(h, axis, g, s, st); break;
     default: el_go<N, BIG>(h, axis, g, s, st); break;
@@ -1545,13 +1534,16 @@ bool fast_plane_available() {
   if (n < 0) n = fast::plane_clusters_per_device();
   return n > 0;
 }
-// Register-order slot -> k_y of the plane pass's y transform (the layout of its multiplier).
-void fast_plane_slot_ky(int Ny, int *ky) {
-  using F = fast::PlaneFY;
-  for (int s = 0; s < Ny; ++s) ky[s] = F::k_of(s % F::G, s / F::G);
+// The plane pass's multiplier layout [kx][slot][j]: tab[slot] = k_y held in register-order
+// slot `slot` of the y transform, tab[Ny + j] = k_z held in position j = t E + idx of the z
+// transform (lane t, register idx).
+void fast_plane_slots(int Ny, int Nz, int *tab) {
+  using F = fast::PlaneF;
+  for (int s = 0; s < Ny; ++s) tab[s] = F::k_of(s % F::G, s / F::G);
+  for (int j = 0; j < Nz; ++j) tab[Ny + j] = F::k_of(j / F::E, j % F::E);
 }
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
-  kwb_launch(fast::k_plane_fast<fast::PlaneFY, fast::PlaneFZ, fast::kPlaneCL>, h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st, h, s);
+  kwb_launch(fast::k_plane_fast<fast::PlaneF, fast::kPlaneCL>, h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st, h, s);
   return cudaGetLastError();
 }
 

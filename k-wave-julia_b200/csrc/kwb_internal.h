@@ -10,6 +10,7 @@
 //     multipliers i k e^{+-i k d/2}/N, PML deficits 1 - pml, and the EOS multiplier
 //     M = [c^2] kappa (1 + nabla1) / (Nx Ny Nz) in the half-spectrum shape.
 #pragma once
+#include <string>
 #include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -37,6 +38,11 @@ struct FftPlan {
   int nstages;
   int radix[KWB_MAX_STAGES];
 };
+
+// Pass slots of the FFT schedule: line passes per axis, the x equation-of-state passes, the
+// y/z spectrum passes.
+enum { KWB_SLOT_LINE0 = 0, KWB_SLOT_LINE1 = 1, KWB_SLOT_LINE2 = 2, KWB_SLOT_EOS_FWD = 3, KWB_SLOT_EOS_INV = 4,
+       KWB_SLOT_SPEC1 = 5, KWB_SLOT_SPEC2 = 6, KWB_NSLOTS = 7 };
 
 // Line-pass modes.
 enum { KWB_MODE_STEP = 0, KWB_MODE_INIT = 1 };
@@ -122,8 +128,8 @@ struct SimDev {
   // nullptr otherwise
   const float *inv_r;
   // 3-D equation of state with the y/z transforms in one cluster pass per kx plane: the half
-  // spectrum is then [z][kx][y] and M is [kx][k_z][slot] (slot: register order of the pass's y
-  // transform, fast_plane_slot_ky)
+  // spectrum is then [z][kx][y] and M is [kx][slot][j] (slot: register order of the pass's y
+  // transform, j: register order of its z transform; fast_plane_slots)
   int plane;
   // the x line pass ends with the equation of state's x R2C (no separate EOS forward pass)
   int fuse_xeos;
@@ -137,6 +143,12 @@ struct SimDev {
 
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
+  // Measured FFT schedule (kwb_tune.cu): register-FFT tile variant per pass slot (KWB_SLOT_*;
+  // -1: the size heuristic) and Stockham line-pass threads per CTA per axis (0: heuristic).
+  // Lines per tile (L_*) and the Stockham radix order (plan) are the other tuned choices.
+  signed char tile_var[8];
+  short thr_line[3];
+  signed char plan_order[3];  // make_plan_order's order of each axis's Stockham plan
   int grid_fill;      // Stockham passes of small grids: narrower tiles and larger CTAs to fill the GPU
 
   // Elastic solver (pstd_elastic_2d/3d).  u[d] are the velocities, p the recorded pressure
@@ -203,10 +215,14 @@ namespace kwb {
 // the complex lines per tile of a line pass (spec = false) or spectrum pass (spec = true) that
 // fit the shared-memory budget, at most cap_lines (kwb_api.cu).
 bool make_plan(int N, FftPlan &pl);
+// The same stages in another order: 0 as make_plan (8s first, then 4 or 2, then 3, 5, 7),
+// 1 radix-4 stages instead of 8s, 2 the odd radices first.
+bool make_plan_order(int N, FftPlan &pl, int order);
 int choose_L(int N, int want, int cap_lines, int dispersion, bool spec);
 size_t line_pass_smem(int N, int L);
 size_t spec_pass_smem(int N, int L, int dispersion);
-int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile);
+// threads per CTA of a Stockham line pass along `axis` (-1: not a line pass)
+int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile, int axis = -1);
 cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
                              long long step_s, cudaStream_t st);
 cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long step_s,
@@ -233,7 +249,8 @@ cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, lo
                       cudaStream_t st);
 bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
-void fast_plane_slot_ky(int Ny, int *ky);
+// Multiplier layout of the plane pass: Ny slot -> k_y entries, then Nz position -> k_z entries.
+void fast_plane_slots(int Ny, int Nz, int *tab);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
 
 // Elastic solver kernels (kwb_elastic.cu).  One gradient pass along `axis` transforms up to
@@ -254,6 +271,34 @@ cudaError_t el_inject(const SimDev &h, int which, long long s, cudaStream_t st);
 cudaError_t el_init(const SimDev &h, cudaStream_t st);
 // Register-FFT gradient pass (kwb_fast.cu) for line lengths 64 ... 1024.
 cudaError_t fast_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
+
+// Post-loop sensor filters (kwb_postfilter.cu): build the FP32 convolution kernels h[nf][Nt] of
+// nf filters (sin_th[f]: sin(theta) of filter f's directivity, NaN for none; freq != 0 adds the
+// Gaussian frequency response), using the FP64 scratch H[nf][Nt] and cosT[Nt]; then filter the
+// series in[t][j] of n_pts points into out with filter fid[j].
+cudaError_t filter_build_kernels(float *h, double *H, double *cosT, int Nt, int nf, const double *sin_th,
+                                 double dir_size, double d_min, double dt, int freq, double fc, double bw,
+                                 cudaStream_t st);
+cudaError_t filter_apply(float *out, const float *in, const float *h, const int *fid, int Nt, long long n_pts,
+                         cudaStream_t st);
+
+// FFT schedule (kwb_tune.cu): the tuned fields of a SimDev.
+struct Schedule {
+  signed char tile_var[8];
+  short thr_line[3];
+  int L_line[3], L_eosx, L_spec[3];
+  signed char plan_order[3];
+};
+void schedule_of(const SimDev &h, Schedule &s);
+void schedule_apply(SimDev &h, const Schedule &s);  // also rebuilds the plans
+std::string schedule_str(const Schedule &s);
+bool schedule_parse(const char *txt, Schedule &s);
+// Measure every pass of h's time step under its candidate schedules (pick >= 0: take candidate
+// `pick` of every pass instead) and store the fastest in h.  Runs on h's own field and spectrum
+// buffers, which the caller must reset afterwards; d_scratch holds the timing descriptor.
+// explore_order adds the Stockham radix orders (not bit-identical to the default order).
+cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pick, bool explore_order,
+                          std::string *log);
 
 // FP64 table builders.
 cudaError_t build_twiddles(float2 *out, int N, cudaStream_t st);

@@ -532,7 +532,8 @@ static int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 // pass launches fewer than four CTAs per SM, so that a small grid's few tiles are not each worked
 // through by 256 threads in long serial loops (the EOS and spectrum passes, shorter per tile,
 // keep 256).
-int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile) {
+int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile, int axis) {
+  if (axis >= 0 && axis < 3 && h.thr_line[axis] > 0) return h.thr_line[axis];
   if (!h.grid_fill || tiles >= 4LL * (h.num_sms > 0 ? h.num_sms : 148)) return KWB_THREADS;
   const long long t = (elems_per_tile / 4 + 31) / 32 * 32;
   return (int)std::min<long long>(KWB_PASS_THREADS_MAX, std::max<long long>(KWB_THREADS, t));
@@ -560,10 +561,10 @@ cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int
   int tiles;
   if (axis == 0) {
     tiles = cdiv(h.N[1], 2 * L) * h.N[2];
-    kwb_launch(k_line_pass<true>, tiles, pass_threads(h, tiles, (long long)L * h.N[0]), sm, st, d_sim, axis, mode, step_s);
+    kwb_launch(k_line_pass<true>, tiles, pass_threads(h, tiles, (long long)L * h.N[0], 0), sm, st, d_sim, axis, mode, step_s);
   } else {
     tiles = cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]);
-    kwb_launch(k_line_pass<false>, tiles, pass_threads(h, tiles, (long long)L * h.N[axis]), sm, st, d_sim, axis, mode,
+    kwb_launch(k_line_pass<false>, tiles, pass_threads(h, tiles, (long long)L * h.N[axis], axis), sm, st, d_sim, axis, mode,
                step_s);
   }
   return cudaGetLastError();

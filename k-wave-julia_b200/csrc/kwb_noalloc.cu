@@ -19,6 +19,7 @@
 //     or processes sharing a device context) race on it and must be serialised by the caller.
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -105,6 +106,8 @@ extern "C" int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t 
   if (nonlinear && !nlq && !std::isfinite(nlq_scalar))
     return fail(KWB_E_INVALID, "nlq_scalar must be finite when nlq is NULL");
   SimDev h{};
+  h.tile_override = -1;
+  memset(h.tile_var, -1, sizeof(h.tile_var));
   h.ndim = h.D = ndim;
   for (int a = 0; a < 3; ++a) {
     const int64_t n = a < ndim ? N_in[a] : 1;

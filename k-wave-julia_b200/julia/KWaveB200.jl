@@ -44,6 +44,12 @@ struct KwbSensorGroup
     cartesian::Int32
     record_mask::UInt32
     record_count::NTuple{13,UInt8}
+    directivity_angle::Ptr{Float64}   # post-loop filters, applied on the device
+    n_directivity_angle::Int64
+    directivity_size::Float64
+    has_frequency_response::Int32
+    frequency_center::Float64
+    frequency_bandwidth::Float64
 end
 struct KwbProblem
     ndim::Int32
@@ -138,6 +144,9 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
                 progress_callback; axisymmetric::Bool=false, elastic::Bool=false)
     (kgrid.Nt[] == 0 || kgrid.dt[] == 0) &&
         error("Time array not set. Call make_time!(kgrid, sound_speed) before running.")
+    data_cast == Float64 && @warn("KWaveB200 steps fields and FFTs in FP32 on the GPU; outputs stay " *
+        "Float64 and agree with the reference's Float64 solve to about 1e-5 relative L2 " *
+        "(data_cast = Float64 is not an FP64 GPU solve)") maxlog = 1
     KWave.validate_record_fields(sensor)
     dims = KWave.grid_size(kgrid)
     D = length(dims)
@@ -183,10 +192,23 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
         if sensor.mask isa AbstractArray{Bool}
             idx = indices(sensor.mask, keep)
             dense = length(idx) == prod(dims)
+            # post-loop filters (first_order_steps.jl:836-910), applied by libkwb before read-back
+            ang_ptr, n_ang, dsize = Ptr{Float64}(C_NULL), Int64(0), 0.0
+            if !elastic && sensor.directivity_angle !== nothing && sensor.directivity_size !== nothing
+                ang = sensor.directivity_angle isa Real ? Float64[sensor.directivity_angle] :
+                      collect(Float64, vec(sensor.directivity_angle))
+                !(sensor.directivity_angle isa Real) && length(ang) < length(idx) &&
+                    throw(BoundsError(sensor.directivity_angle, length(idx)))   # angle[j], first_order_steps.jl:853
+                push!(keep, ang)
+                ang_ptr, n_ang, dsize = pointer(ang), Int64(length(ang)), Float64(sensor.directivity_size)
+            end
+            has_fr = !elastic && sensor.frequency_response !== nothing
+            fc, bw = has_fr ? Float64.(sensor.frequency_response) : (0.0, 0.0)
             push!(groups, KwbSensorGroup(dense ? C_NULL : pointer(idx), length(idx), Int32(dense), 0,
-                                         mask, Tuple(counts)))
+                                         mask, Tuple(counts), ang_ptr, n_ang, dsize, Int32(has_fr), fc, bw))
         else
-            push!(groups, KwbSensorGroup(C_NULL, size(sensor.mask, 2), 0, 1, mask, Tuple(counts)))
+            push!(groups, KwbSensorGroup(C_NULL, size(sensor.mask, 2), 0, 1, mask, Tuple(counts),
+                                         C_NULL, 0, 0.0, 0, 0.0, 0.0))
         end
     end
     push!(keep, groups)
@@ -262,10 +284,8 @@ function _solve(kgrid, medium, source, sensor, pml_size, pml_alpha, smooth_p0, d
         kgrid.Nt[] = size(sensor.time_reversal_boundary_data, 2)   # first_order.jl:430-431
         data[:p_final] = pfull
     end
-    if !elastic  # the elastic solvers return the recorded data as it is
-        KWave.apply_sensor_directivity!(data, sensor, kgrid)        # host post-filters, as the
-        KWave.apply_frequency_response!(data, sensor, kgrid)        # reference runs them
-    end
+    # the post-loop filters (apply_sensor_directivity!, apply_frequency_response!) ran in libkwb
+    # on the device before read-back; the elastic solvers have none
     return KWave.SimulationOutput(data)
 end
 

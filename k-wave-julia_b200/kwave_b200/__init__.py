@@ -12,7 +12,7 @@ from .core import (Additive, AdditiveNoCorrection, Dirichlet, ElasticMedium, Ela
                    make_time, neper2db, smooth, tone_burst, validate_record_fields)
 from ._lib import KWaveB200Error, LIB_PATH, load_library
 from .solver import (Context, Prepared, Request, Simulation, prepare, solve_prepared, submit_prepared, build_problem, default_context, estimate_device_bytes,
-                     kspace_first_order, kspace_first_order_as, pstd_elastic_2d, pstd_elastic_3d, serving_config, serving_stats, shard_jobs, solve_batch, submit)
+                     kspace_first_order, kspace_first_order_as, pstd_elastic_2d, pstd_elastic_3d, run_sharded, serving_config, serving_stats, shard_jobs, solve_batch, submit)
 
 make_time_ = make_time  # `make_time!` in the reference
 
@@ -23,7 +23,7 @@ __all__ = [
     "make_time", "make_time_", "neper2db", "smooth", "tone_burst", "validate_record_fields",
     "KWaveB200Error", "LIB_PATH", "load_library", "Context", "Simulation", "build_problem",
     "default_context", "kspace_first_order", "kspace_first_order_as", "Request", "estimate_device_bytes", "serving_config",
-    "serving_stats", "shard_jobs", "solve_batch", "submit", "Prepared", "prepare", "solve_prepared",
+    "serving_stats", "shard_jobs", "run_sharded", "solve_batch", "submit", "Prepared", "prepare", "solve_prepared",
     "submit_prepared", "ElasticMedium", "ElasticSource", "pstd_elastic_2d", "pstd_elastic_3d",
     "grid_size", "grid_spacing", "k_max", "total_grid_points",
 ]

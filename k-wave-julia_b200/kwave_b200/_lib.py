@@ -52,7 +52,10 @@ class Signal(C.Structure):
 class SensorGroup(C.Structure):
     _fields_ = [("index", C.POINTER(C.c_int64)), ("n_index", C.c_int64), ("dense", C.c_int32),
                 ("cartesian", C.c_int32), ("record_mask", C.c_uint32),
-                ("record_count", C.c_uint8 * REC_COUNT)]
+                ("record_count", C.c_uint8 * REC_COUNT),
+                ("directivity_angle", C.POINTER(C.c_double)), ("n_directivity_angle", C.c_int64),
+                ("directivity_size", C.c_double), ("has_frequency_response", C.c_int32),
+                ("frequency_center", C.c_double), ("frequency_bandwidth", C.c_double)]
 
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_int64, C.c_int64, C.POINTER(C.c_float), C.c_void_p)
@@ -111,7 +114,7 @@ EXPORTS = (
     "kwb_version", "kwb_context_create", "kwb_context_destroy", "kwb_last_error",
     "kwb_query_outputs", "kwb_solve", "kwb_sim_create", "kwb_sim_advance",
     "kwb_sim_advance_timed", "kwb_sim_steps_done", "kwb_sim_sync", "kwb_sim_read_outputs",
-    "kwb_sim_read_pressure", "kwb_sim_destroy", "kwb_sim_profile", "kwb_sim_info",
+    "kwb_sim_read_pressure", "kwb_sim_destroy", "kwb_sim_profile", "kwb_sim_info", "kwb_sim_schedule",
 )
 
 _lib = None
@@ -162,6 +165,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         lib.kwb_sim_profile.argtypes = [vp, C.c_int64, C.POINTER(KernelTimes)]
         lib.kwb_sim_info.restype = C.c_int
         lib.kwb_sim_info.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        lib.kwb_sim_schedule.restype = C.c_int
+        lib.kwb_sim_schedule.argtypes = [vp, C.c_char_p, C.c_int64]
         lib.kwb_estimate_device_bytes.restype = C.c_int
         lib.kwb_estimate_device_bytes.argtypes = [vp, C.POINTER(Problem), C.POINTER(C.c_int64)]
         lib.kwb_serving_config.restype = C.c_int

@@ -19,8 +19,8 @@ invalid record field, signals with too few rows (BoundsError), ``:I_avg``/``:I_m
 from __future__ import annotations
 
 import ctypes as C
-import math
 import threading
+import warnings
 from typing import Optional
 
 import numpy as np
@@ -136,6 +136,14 @@ class _Built:
     def arr(self, a):
         self.keep.append(a)
         return a
+
+
+def _warn_fp32(data_cast):
+    """The reference's default data_cast=Float64 asks for an FP64 solve; this path steps in FP32."""
+    if np.dtype(data_cast) == np.float64:
+        warnings.warn("kwave_b200 steps fields and FFTs in FP32 on the GPU; outputs stay float64 and agree "
+                      "with the reference's Float64 solve to about 1e-5 relative L2 (data_cast=float64 is "
+                      "not an FP64 GPU solve)", RuntimeWarning, stacklevel=3)
 
 
 def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, sensor: KWaveSensor,
@@ -308,6 +316,22 @@ def build_problem(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource, se
         for f in rec:
             g.record_mask |= 1 << _lib.REC[f]
             g.record_count[_lib.REC[f]] += 1
+        if gi == 0 and not elastic and m.dtype == bool:
+            # post-loop filters of p (first_order_steps.jl:836-910), applied by the library on the
+            # device before read-back; the elastic solvers have none
+            if sen.directivity_angle is not None and sen.directivity_size is not None:
+                ang = np.asarray(sen.directivity_angle, dtype=np.float64)
+                flat = b.arr(np.ascontiguousarray(ang.ravel(order="F")))
+                if ang.ndim > 0 and flat.size < n_rows:
+                    raise IndexError(f"BoundsError: directivity_angle has {flat.size} entries for {n_rows} sensor points")
+                g.directivity_angle = _ptr_d(flat)
+                g.n_directivity_angle = 1 if ang.ndim == 0 else flat.size
+                g.directivity_size = float(sen.directivity_size)
+            if sen.frequency_response is not None:
+                fc, bw = sen.frequency_response
+                g.has_frequency_response = 1
+                g.frequency_center = float(fc)
+                g.frequency_bandwidth = float(bw)
         groups.append(g)
         b.groups_py.append((rec, n_rows, bool(g.cartesian)))
     if groups:
@@ -398,49 +422,9 @@ def _collect(b: _Built, arrays, pfull, sensor: KWaveSensor, kgrid: KWaveGrid, Nt
     extra = dicts[1:] if sensor.mask is not None else dicts
     if pfull is not None:
         main["p_final"] = pfull
-    if not b.problem.elastic:  # the elastic solvers return the recorded data as it is
-        apply_sensor_directivity(main, sensor, kgrid)
-        apply_frequency_response(main, sensor, kgrid)
     out = SimulationOutput(main)
     out.extra = extra
     return out
-
-
-_FILTER_ROWS = 4096  # sensor rows transformed at once by the post-loop filters (bounds memory)
-
-
-def apply_sensor_directivity(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
-    """first_order_steps.jl:836-873 -- per-sensor sinc(k a sin(theta)/2) filter of p (host, FP64),
-    all sensors with a non-zero angle at once (rows with angle 0 are left as they are)."""
-    if sensor.directivity_angle is None or sensor.directivity_size is None or "p" not in data:
-        return
-    p = data["p"]
-    n, Nt = p.shape
-    freqs = np.fft.fftfreq(Nt, kgrid.dt)
-    dmin = kgrid.d[0] if kgrid.ndim == 1 else min(kgrid.d)
-    ang = np.asarray(sensor.directivity_angle, dtype=np.float64)
-    th = np.full(n, float(ang)) if ang.ndim == 0 else ang.ravel()[:n]
-    kval = 2 * math.pi * np.abs(freqs) / dmin
-    rows = np.flatnonzero(th != 0.0)  # `angle ≈ 0` with default tolerances holds only for 0
-    for lo in range(0, rows.size, _FILTER_ROWS):
-        r = rows[lo: lo + _FILTER_ROWS]
-        arg = kval[None, :] * sensor.directivity_size * np.sin(th[r])[:, None] / 2
-        with np.errstate(invalid="ignore", divide="ignore"):
-            filt = np.where(arg == 0, 1.0, np.sin(arg) / np.where(arg == 0, 1.0, arg))
-        p[r, :] = np.real(np.fft.ifft(np.fft.fft(p[r, :], axis=1) * filt, axis=1))
-
-
-def apply_frequency_response(data: dict, sensor: KWaveSensor, kgrid: KWaveGrid):
-    """first_order_steps.jl:880-910 -- Gaussian band-pass of p (host, FP64), all sensors at once."""
-    if sensor.frequency_response is None or "p" not in data:
-        return
-    fc, bw = sensor.frequency_response
-    p = data["p"]
-    n, Nt = p.shape
-    resp = np.exp(-((np.abs(np.fft.fftfreq(Nt, kgrid.dt)) - fc) ** 2) / (2 * bw ** 2))
-    for lo in range(0, n, _FILTER_ROWS):
-        p[lo: lo + _FILTER_ROWS, :] = np.real(np.fft.ifft(np.fft.fft(p[lo: lo + _FILTER_ROWS, :], axis=1) * resp,
-                                                          axis=1))
 
 
 def kspace_first_order(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSource,
@@ -457,6 +441,7 @@ def kspace_first_order(kgrid: KWaveGrid, medium: KWaveMedium, source: KWaveSourc
     FFTs are FP32 whatever ``data_cast`` says; ``data_cast`` only selects the reference's error
     behaviour for ``:I_avg``/``:I_max``.
     """
+    _warn_fp32(data_cast)
     if save_to_disk is not None:
         raise NotImplementedError("save_to_disk writes an HDF5 input file for the k-Wave C++ binary; "
                                   "HDF5 output is not part of this library")
@@ -582,6 +567,13 @@ class Simulation:
         nl = C.c_int32(0)
         self._chk(self.ctx.lib.kwb_sim_info(self.handle, C.byref(nb), C.byref(nl)))
         return {"device_bytes": nb.value, "launches_per_step": nl.value}
+
+    def schedule(self) -> str:
+        """The FFT schedule of this simulation's time step: "tuned" (measured on first use of the
+        grid shape), "cache" (an earlier measurement) or "heuristic", then the per-pass choices."""
+        buf = C.create_string_buffer(512)
+        self._chk(self.ctx.lib.kwb_sim_schedule(self.handle, buf, len(buf)))
+        return buf.value.decode()
 
     def close(self):
         if getattr(self, "handle", None):
@@ -716,6 +708,75 @@ def solve_batch(jobs, context: Optional[Context] = None) -> list:
     """Run many independent simulations together; jobs are (kgrid, medium, source, sensor, kwargs)."""
     reqs = [submit(g, m, s, sen, context=context, **kw) for g, m, s, sen, kw in jobs]
     return [r.result() for r in reqs]
+
+
+def _job_parts(job):
+    """(kgrid, medium, source, sensor, keyword arguments) of one batch entry."""
+    if len(job) == 5:
+        return job
+    kgrid, medium, source, sensor = job
+    return kgrid, medium, source, sensor, {}
+
+
+def run_sharded(jobs, *, world: Optional[int] = None, rank: Optional[int] = None, devices=None,
+                runner=None) -> dict:
+    """Run a batch of independent simulations over several GPUs; returns {job index: output}
+    for the jobs this process ran.
+
+    ``jobs`` is a list of ``(kgrid, medium, source, sensor)`` or ``(..., kwargs)`` entries, the
+    arguments of one ``kspace_first_order`` call each.  Jobs are assigned longest first to the
+    least-loaded GPU by voxels x steps (``shard_jobs``); simulations are independent, so GPUs
+    exchange nothing while they run and the results come together on the host.
+
+    * One process per GPU (torchrun): ``world``/``rank`` (default: torch.distributed's, else 1/0)
+      select this process's share, run on device LOCAL_RANK (or ``devices[0]``).
+    * One process, several GPUs: ``devices=[0, 1, ...]`` runs every share, one host thread and
+      one context per device.
+
+    Each device runs its share through the continuous-batching scheduler (``submit``).
+    ``runner(device, built_problems)`` replaces the library call (tests without a GPU)."""
+    if world is None or rank is None:
+        try:
+            import torch.distributed as dist
+            ok = dist.is_available() and dist.is_initialized()
+        except Exception:
+            ok = False
+        world = dist.get_world_size() if ok else 1
+        rank = dist.get_rank() if ok else 0
+    parts = [_job_parts(j) for j in jobs]
+    costs = [int(np.prod(g.N)) * int(g.Nt) for g, *_ in parts]
+
+    def run_on(device, idx):
+        if runner is not None:
+            built = [build_problem(*parts[i][:4], **{k: v for k, v in parts[i][4].items()
+                                                     if k in ("pml_size", "pml_alpha", "smooth_p0")})
+                     for i in idx]
+            return dict(zip(idx, runner(device, built)))
+        ctx = Context(device)
+        reqs = [submit(*parts[i][:4], context=ctx, **parts[i][4]) for i in idx]
+        return {i: r.result() for i, r in zip(idx, reqs)}
+
+    if devices is not None and len(devices) > 1 and world == 1:
+        shares = [shard_jobs(costs, len(devices), r) for r in range(len(devices))]
+        out, errs = {}, []
+
+        def work(r):
+            try:
+                out.update(run_on(devices[r], shares[r]))
+            except BaseException as e:  # re-raised on the calling thread
+                errs.append(e)
+
+        threads = [threading.Thread(target=work, args=(r,)) for r in range(len(devices))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errs:
+            raise errs[0]
+        return out
+    import os
+    device = devices[0] if devices else int(os.environ.get("LOCAL_RANK", "0"))
+    return run_on(device, shard_jobs(costs, world, rank))
 
 
 def shard_jobs(costs, world: int, rank: int) -> list:

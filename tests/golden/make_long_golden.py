@@ -14,7 +14,7 @@ Inputs come from the seeded workload builders (``kwave_b200.workloads``), so the
                 ``p``: their pressure series [1024 x 1500]; ``vol_idx``: every 4th voxel along
                 each axis (offset 1), ``p_max``: the volume p_max there [262144].
 * c2_long.npz   ``p_max``, ``p_rms``: the full-grid aggregates [262144] each.
-* serving_sample.npz  for every 16th request of the 48-request serving stream (Nt 300-800,
+* serving_sample.npz  for requests 0, 16 and 22 of the 48-request serving stream (Nt 300-800,
                 seed 5005): its 16-point sensor line's p series.
 
 Indices are column-major (Julia) linear indices, the order the reference's ``findall`` returns.
@@ -30,10 +30,10 @@ ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "k-wave-julia_b200"),
                 os.path.join(ROOT, "tests")]
 
-# serving stream sampled for per-request accuracy (every 16th of the 48 requests)
+# serving stream sampled for per-request accuracy: two 2D requests and one 3D request of the 48
 SERVING_SEED = 5005
 SERVING_NT = (300, 800)
-SERVING_SAMPLE = (0, 16, 32)
+SERVING_SAMPLE = (0, 16, 22)
 
 
 def c3_samples(n=256):

@@ -37,7 +37,8 @@ def test_struct_layouts_match_header():
 #include <stddef.h>
 #include "kwb.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(kwb_problem), sizeof(kwb_sensor_group),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(kwb_problem), sizeof(kwb_sensor_group),
+         offsetof(kwb_sensor_group, directivity_angle), offsetof(kwb_sensor_group, frequency_bandwidth),
          offsetof(kwb_problem, groups), offsetof(kwb_problem, tr), offsetof(kwb_problem, u_signal),
          sizeof(kwb_kernel_times), sizeof(kwb_group_sizes), sizeof(kwb_outputs), offsetof(kwb_problem, p0),
          offsetof(kwb_problem, elastic), offsetof(kwb_problem, cs), offsetof(kwb_problem, alpha_coeff_shear),
@@ -49,7 +50,8 @@ int main(void) {
         open(cpath, "w").write(prog)
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), cpath, "-o", exe], check=True)
         got = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
-    exp = [C.sizeof(L.Problem), C.sizeof(L.SensorGroup), L.Problem.groups.offset, L.Problem.tr.offset,
+    exp = [C.sizeof(L.Problem), C.sizeof(L.SensorGroup), L.SensorGroup.directivity_angle.offset,
+           L.SensorGroup.frequency_bandwidth.offset, L.Problem.groups.offset, L.Problem.tr.offset,
            L.Problem.u_signal.offset, C.sizeof(L.KernelTimes), C.sizeof(L.GroupSizes), C.sizeof(L.Outputs),
            L.Problem.p0.offset, L.Problem.elastic.offset, L.Problem.cs.offset,
            L.Problem.alpha_coeff_shear.offset, L.Problem.s_signal.offset]

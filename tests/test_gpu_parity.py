@@ -298,6 +298,38 @@ def test_duplicate_record_and_short_signal(kb):
     assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
 
 
+@pytest.mark.parametrize("Nt,angles", [(300, "array"), (257, "scalar")])
+def test_post_filters_on_the_device(kb, Nt, angles):
+    """Sensor directivity and frequency response (first_order_steps.jl:836-910) run in libkwb on
+    the recorded series before read-back: per-point angles (some exactly 0, which skip the
+    directivity) or one scalar angle, odd and even series lengths; against the oracle's FFT
+    filters on its own FP64 solve."""
+    from kwave_b200.workloads import Case
+    n = 64
+    p_mask = kb.make_disc(n, n, 30, 34, 3)
+    t = np.arange(Nt) * (0.3e-4 / 1500)
+    sig = np.vstack([np.sin(2 * math.pi * 1.5e6 * t) * np.exp(-((t - 1e-6) / 4e-7) ** 2)] * int(p_mask.sum()))
+    mask = np.zeros((n, n), bool)
+    mask[12, 8:56:3] = True
+    mask[44, 10:50:4] = True
+    npts = int(mask.sum())
+    ang = np.linspace(-1.0, 1.2, npts)
+    ang[[0, 7]] = 0.0
+    sensor = dict(mask=mask, record=["p", "p_max"], directivity_angle=ang if angles == "array" else 0.6,
+                  directivity_size=3e-4, frequency_response=(1.2e6, 6e5))
+    case = Case("filters", (n, n), (1e-4, 1e-4), 0.3e-4 / 1500, Nt,
+                dict(sound_speed=1500.0, density=1000.0), dict(p_mask=p_mask, p=sig), sensor, pml_size=10)
+    g, r = run_gpu(case), run_oracle(case)
+    rep = {}
+    assert_parity(g, r, TOL_L2, TOL_MAX, report=rep)
+    print("filters", angles, rep)
+    # the filters changed the series (p_max is recorded unfiltered, as in the reference)
+    unf = run_gpu(Case("unfiltered", case.N, case.d, case.dt, Nt, case.medium, case.source,
+                       dict(mask=mask, record=["p", "p_max"]), pml_size=10))
+    assert np.linalg.norm(unf["p"] - g["p"]) > 1e-3 * np.linalg.norm(unf["p"])
+    assert np.array_equal(unf["p_max"], g["p_max"])
+
+
 def test_graph_replay_matches_eager_chunks(kb, wl):
     """CUDA-graph replay of 32-step chunks gives bit-identical fields to eager single steps."""
     case = wl.c2(n=96, Nt=100, record=("p_max",))

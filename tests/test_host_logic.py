@@ -128,36 +128,66 @@ def test_findall_sparse_and_dense_paths_agree():
     assert b.problem.groups[0].dense == 1 and b.problem.groups[0].n_index == 48
 
 
-def test_post_filters_match_the_oracle_per_row():
-    """Sensor directivity and frequency response (first_order_steps.jl:836-910), applied to all
-    rows at once on the host, equal the oracle's row-by-row restatement; rows whose angle is 0
-    are untouched."""
-    import sys
+def test_post_filter_convolution_form_matches_the_oracle():
+    """The device post-filters (kwb_postfilter.cu) apply the reference's
+    real(ifft(fft(p) .* H)) as a circular convolution with h = ifft(H), H real and even in |f|
+    (first_order_steps.jl:836-910).  Restated here in NumPy on the same steps -- H per distinct
+    angle, h by an FP64 cosine sum, p' = h (*) p -- it equals the oracle's FFT filters; rows
+    whose angle is 0 get the frequency response only."""
     import kwave_ref as K
-    from kwave_b200.solver import apply_frequency_response, apply_sensor_directivity
-    import kwave_b200 as kb
     rng = np.random.default_rng(3)
-    n, Nt = 37, 211
-    g = kb.KWaveGrid(32, 1e-4, 24, 2e-4)
-    g.dt = 2e-8
-    go = K.KWaveGrid(32, 1e-4, 24, 2e-4)
-    go.dt = 2e-8
-    ang = rng.uniform(-1.2, 1.2, n)
-    ang[[0, 5, 9]] = 0.0
-    p = rng.standard_normal((n, Nt))
-    sen = kb.KWaveSensor(mask=np.ones((32, 24), bool), record=["p"])
-    sen.directivity_angle, sen.directivity_size, sen.frequency_response = ang, 3e-4, (2e6, 8e5)
-    seno = K.KWaveSensor(mask=np.ones((32, 24), bool), record=["p"])
-    seno.directivity_angle, seno.directivity_size, seno.frequency_response = ang, 3e-4, (2e6, 8e5)
-    a, b = {"p": p.copy()}, {"p": p.copy()}
-    apply_sensor_directivity(a, sen, g)
-    apply_frequency_response(a, sen, g)
-    K.apply_sensor_directivity(b, seno, go)
-    K.apply_frequency_response(b, seno, go)
-    assert np.allclose(a["p"], b["p"], rtol=0, atol=1e-12 * np.abs(b["p"]).max())
-    d = {"p": p.copy()}
-    apply_sensor_directivity(d, sen, g)
-    assert np.array_equal(d["p"][[0, 5, 9]], p[[0, 5, 9]])
+    for n, Nt in ((37, 211), (5, 64), (9, 1)):
+        dt = 2e-8
+        go = K.KWaveGrid(32, 1e-4, 24, 2e-4)
+        go.dt = dt
+        ang = rng.uniform(-1.2, 1.2, n)
+        ang[[0, n // 2]] = 0.0
+        p = rng.standard_normal((n, Nt))
+        seno = K.KWaveSensor(mask=np.ones((32, 24), bool), record=["p"])
+        seno.directivity_angle, seno.directivity_size, seno.frequency_response = ang, 3e-4, (2e6, 8e5)
+        b = {"p": p.copy()}
+        K.apply_sensor_directivity(b, seno, go)
+        K.apply_frequency_response(b, seno, go)
+        k = np.arange(Nt)
+        f = np.where(k < (Nt + 1) // 2, k, k - Nt) / (Nt * dt)
+        af = np.abs(f)
+        out = np.empty_like(p)
+        cosT = np.cos(2 * np.pi * np.arange(Nt) / Nt)
+        for j in range(n):
+            H = np.exp(-((af - 2e6) ** 2) / (2 * (8e5) ** 2))
+            if ang[j] != 0.0:
+                arg = 2 * np.pi * af / 1e-4 * 3e-4 * np.sin(ang[j]) / 2
+                H = H * np.where(arg == 0, 1.0, np.sin(arg) / np.where(arg == 0, 1.0, arg))
+            h = np.array([np.dot(H, cosT[(k * m) % Nt]) for m in range(Nt)]) / Nt
+            out[j] = [np.dot(h[(m - k) % Nt], p[j]) for m in range(Nt)]
+        assert np.allclose(out, b["p"], rtol=0, atol=1e-12 * max(1.0, np.abs(b["p"]).max())), (n, Nt)
+
+
+def test_build_problem_carries_post_filters():
+    """The sensor's directivity and frequency response reach the first sensor group of the ABI
+    problem (applied by the library on the device); angle arrays in column-major order, scalar
+    angles as one value for every point, short arrays raise as the reference's angle[j] would."""
+    g = kb.KWaveGrid(8, 1e-4, 6, 1e-4)
+    kb.make_time(g, 1500.0, t_end=1e-6)
+    med, src = kb.KWaveMedium(sound_speed=1500.0), kb.KWaveSource(p0=np.ones((8, 6)))
+    m = np.zeros((8, 6), bool)
+    m[2, 1:4] = True
+    ang = np.array([0.1, 0.0, 0.3])
+    sen = kb.KWaveSensor(mask=m, record=["p"], directivity_angle=ang, directivity_size=2e-4,
+                         frequency_response=(1e6, 3e5))
+    b = kb.build_problem(g, med, src, sen)
+    grp = b.problem.groups[0]
+    assert grp.n_directivity_angle == 3 and grp.directivity_size == 2e-4
+    assert [grp.directivity_angle[i] for i in range(3)] == [0.1, 0.0, 0.3]
+    assert grp.has_frequency_response == 1 and (grp.frequency_center, grp.frequency_bandwidth) == (1e6, 3e5)
+    sen1 = kb.KWaveSensor(mask=m, record=["p"], directivity_angle=0.5, directivity_size=2e-4)
+    grp1 = kb.build_problem(g, med, src, sen1).problem.groups[0]
+    assert grp1.n_directivity_angle == 1 and grp1.has_frequency_response == 0
+    with pytest.raises(IndexError):
+        kb.build_problem(g, med, src, kb.KWaveSensor(mask=m, record=["p"], directivity_angle=ang[:2],
+                                                     directivity_size=2e-4))
+    nofilt = kb.build_problem(g, med, src, kb.KWaveSensor(mask=m, record=["p"])).problem.groups[0]
+    assert not nofilt.directivity_angle and nofilt.has_frequency_response == 0
 
 
 def test_build_problem_elastic():
