@@ -36,7 +36,8 @@ extern "C" {
 enum kwb_status {
   KWB_OK = 0,
   KWB_E_INVALID = -1,     /* malformed problem (the reference's error(...) / BoundsError cases) */
-  KWB_E_UNSUPPORTED = -2, /* valid for the reference but outside this library (e.g. a grid side with a prime factor > 7) */
+  KWB_E_UNSUPPORTED = -2, /* valid for the reference but outside this library (a grid side above 4096, or
+                             above 2048 with a prime factor > 7) */
   KWB_E_NOMEM = -3,       /* device memory admission failed */
   KWB_E_DEVICE = -4,      /* CUDA error or a device-side bounded wait that gave up */
   KWB_E_TIMEOUT = -5,     /* kwb_wait() deadline passed */

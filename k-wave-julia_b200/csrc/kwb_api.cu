@@ -178,6 +178,73 @@ bool make_plan_order(int N, FftPlan &pl, int order) {
 
 bool make_plan(int N, FftPlan &pl) { return make_plan_order(N, pl, 0); }
 
+bool plan_line(int N, FftPlan &pl, int order) {
+  const float2 *chirp = pl.chirp, *chirp_ft = pl.chirp_ft;  // tables built by the caller
+  pl.m = 0;
+  if (!make_plan_order(N, pl, order)) {
+    if (N > KWB_BLUESTEIN_MAX_N) return false;
+    int M = 1;
+    while (M < 2 * N - 1) M *= 2;
+    if (!make_plan_order(M, pl, order)) return false;
+    pl.n = N;
+    pl.m = M;
+  }
+  pl.chirp = chirp;
+  pl.chirp_ft = chirp_ft;
+  return true;
+}
+
+// Bluestein tables of an n-point line with inner length m (FP64, rounded once): the chirp
+// w_j = exp(-i pi j^2/n) (j^2 reduced mod 2n exactly, in integers) and FFT_m of its conjugate
+// wrapped to length m (b_j = b_{m-j} = conj(w_j), j < n), scaled by 1/m.
+void bluestein_tables(int n, int m, std::vector<float2> &chirp, std::vector<float2> &chirp_ft) {
+  const double pi = 3.141592653589793238462643;
+  std::vector<double> wr(n), wi(n);
+  for (int j = 0; j < n; ++j) {
+    const long long q = ((long long)j * j) % (2LL * n);
+    const double th = pi * (double)q / (double)n;
+    wr[j] = std::cos(th);
+    wi[j] = -std::sin(th);
+  }
+  std::vector<double> br(m, 0.0), bi(m, 0.0);
+  for (int j = 0; j < n; ++j) {
+    br[j] = wr[j];
+    bi[j] = -wi[j];
+    if (j > 0) {
+      br[m - j] = wr[j];
+      bi[m - j] = -wi[j];
+    }
+  }
+  // iterative radix-2 FFT (forward, exp(-2 pi i jk/m)), m a power of two
+  for (int i = 1, j = 0; i < m; ++i) {
+    int bit = m >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(br[i], br[j]);
+      std::swap(bi[i], bi[j]);
+    }
+  }
+  for (int len = 2; len <= m; len <<= 1) {
+    for (int k = 0; k < len / 2; ++k) {
+      const double a = -2.0 * pi * (double)k / (double)len;
+      const double cr = std::cos(a), ci = std::sin(a);
+      for (int i = 0; i < m; i += len) {
+        const int u = i + k, v = i + k + len / 2;
+        const double tr = br[v] * cr - bi[v] * ci, ti = br[v] * ci + bi[v] * cr;
+        br[v] = br[u] - tr;
+        bi[v] = bi[u] - ti;
+        br[u] += tr;
+        bi[u] += ti;
+      }
+    }
+  }
+  chirp.resize(n);
+  chirp_ft.resize(m);
+  for (int j = 0; j < n; ++j) chirp[j] = make_float2((float)wr[j], (float)wi[j]);
+  for (int k = 0; k < m; ++k) chirp_ft[k] = make_float2((float)(br[k] / m), (float)(bi[k] / m));
+}
+
 int choose_L(int N, int want, int cap_lines, int dispersion, bool spec) {
   int L = want;
   if (L < 1) L = 1;
@@ -322,11 +389,12 @@ int validate_problem(kwb_ctx *ctx, const kwb_problem *P) {
     if (n < 1) return set_err(ctx, KWB_E_INVALID, "grid size N[%d] = %lld must be >= 1", a, (long long)n);
     if (n > KWB_MAX_N)
       return set_err(ctx, KWB_E_UNSUPPORTED, "grid size N[%d] = %lld exceeds %d", a, (long long)n, KWB_MAX_N);
-    FftPlan pl;
-    if (!make_plan((int)n, pl))
+    FftPlan pl{};
+    if (!plan_line((int)n, pl, 0))
       return set_err(ctx, KWB_E_UNSUPPORTED,
-                     "grid size N[%d] = %lld has a prime factor above 7 (the FFT engine supports "
-                     "radices 2, 3, 5 and 7)", a, (long long)n);
+                     "grid size N[%d] = %lld has a prime factor above 7 and exceeds %d, the longest "
+                     "line transformed by Bluestein's algorithm (radix 2, 3, 5, 7 lengths up to %d)",
+                     a, (long long)n, KWB_BLUESTEIN_MAX_N, KWB_MAX_N);
     if (a < P->ndim && !(P->d[a] > 0)) return set_err(ctx, KWB_E_INVALID, "grid spacing d[%d] must be > 0", a);
     nvox *= n;
   }
@@ -933,11 +1001,13 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
 
   // ---- tile shapes and FFT plans
   CU(cudaDeviceGetAttribute(&h.num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
-  for (int a = 0; a < 3; ++a) make_plan(h.N[a], h.plan[a]);
-  h.L_line[0] = choose_L(h.N[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, 0, false);
-  for (int a = 1; a < 3; ++a) h.L_line[a] = choose_L(h.N[a], 8, (h.N[0] + 1) / 2, 0, false);
-  h.L_eosx = choose_L(h.N[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, h.dispersion, true);
-  for (int a = 1; a < 3; ++a) h.L_spec[a] = choose_L(h.N[a], 8, h.n1, h.dispersion, true);
+  for (int a = 0; a < 3; ++a) plan_line(h.N[a], h.plan[a], 0);
+  int FL[3];  // transform length per axis (the Bluestein inner length where there is one)
+  for (int a = 0; a < 3; ++a) FL[a] = fft_len(h.plan[a]);
+  h.L_line[0] = choose_L(FL[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, 0, false);
+  for (int a = 1; a < 3; ++a) h.L_line[a] = choose_L(FL[a], 8, (h.N[0] + 1) / 2, 0, false);
+  h.L_eosx = choose_L(FL[0], std::max(1, 2048 / h.N[0]), (h.N[1] + 1) / 2, h.dispersion, true);
+  for (int a = 1; a < 3; ++a) h.L_spec[a] = choose_L(FL[a], 8, h.n1, h.dispersion, true);
   h.L_spec[0] = 1;
   {
     // A simulation that runs alone gets narrower tiles and larger CTAs on small grids (latency:
@@ -1110,14 +1180,26 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   // ---- per-axis tables (FP64 on device)
   for (int a = 0; a < 3; ++a) {
     const int n = h.N[a];
+    const int nt = fft_len(h.plan[a]);  // twiddles of the transform length
     float2 *tw, *gp, *gn;
     float *pd, *psd;
-    CU(M.alloc(&tw, n));
+    CU(M.alloc(&tw, nt));
     CU(M.alloc(&gp, n));
     CU(M.alloc(&gn, n));
     CU(M.alloc(&pd, n));
     CU(M.alloc(&psd, n));
-    CU(build_twiddles(tw, n, st));
+    CU(build_twiddles(tw, nt, st));
+    if (h.plan[a].m > 0) {
+      std::vector<float2> ch, chf;
+      bluestein_tables(n, h.plan[a].m, ch, chf);
+      float2 *dch, *dchf;
+      CU(M.alloc(&dch, ch.size()));
+      CU(M.alloc(&dchf, chf.size()));
+      if ((rc = upload(ctx, dch, ch.data(), ch.size() * sizeof(float2), st))) return rc;
+      if ((rc = upload(ctx, dchf, chf.data(), chf.size() * sizeof(float2), st))) return rc;
+      h.plan[a].chirp = dch;
+      h.plan[a].chirp_ft = dchf;
+    }
     const double d = a < D ? P->d[a] : 1.0;
     CU(build_gradient(gp, gn, n, d, st));
     const int psz = a < D ? (int)P->pml_size[a] : 0;
@@ -1160,9 +1242,9 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (h.dispersion) CU(M.alloc(&M2, h.nspec));
     int *slot_ky = nullptr;
     if (h.plane) {
-      std::vector<int> ky(h.N[1] + h.N[2]);
-      fast_plane_slots(h.N[1], h.N[2], ky.data());
-      CU(M.alloc(&slot_ky, ky.size()));
+      std::vector<int> ky(h.N[1]);
+      fast_plane_slot_ky(h.N[1], ky.data());
+      CU(M.alloc(&slot_ky, h.N[1]));
       if ((rc = upload(ctx, slot_ky, ky.data(), ky.size() * sizeof(int), st))) return rc;
     }
     const double d3[3] = {P->d[0], D > 1 ? P->d[1] : 1.0, D > 2 ? P->d[2] : 1.0};

@@ -55,12 +55,12 @@ __global__ void __launch_bounds__(KWB_PASS_THREADS_MAX)
   extern __shared__ float4 smem_raw[];
   const int N = S.N[axis];
   const int L = S.L_line[axis];
-  const int LS = line_pitch(N);
+  const int LS = line_pitch(fft_len(S.plan[axis]));
   const int Nx = S.N[0];
   float2 *X = reinterpret_cast<float2 *>(smem_raw);
   float2 *Y = X + L * LS;
   float2 *tw = Y + L * LS;
-  load_twiddles(tw, S.tw[axis], N);  // set-up-time table: before waiting on the previous kernel
+  load_twiddles(tw, S.tw[axis], fft_len(S.plan[axis]));  // set-up-time table: before waiting on the previous kernel
   KWB_STEP_KERNEL_PROLOGUE();
   if (step_index(S, step_s) >= S.Nt) return;
   const Tile T = CONTIG ? tile_x(S, 2 * L, blockIdx.x) : tile_yz(S, axis, 2 * L, blockIdx.x);
@@ -386,9 +386,9 @@ static bool el_fast(const SimDev &h, int axis) {
 }
 
 cudaError_t el_prime(const SimDev &h) {
-  cudaError_t e = set_smem_optin((const void *)k_el_grad<true>, line_pass_smem(h.N[0], h.L_line[0]));
+  cudaError_t e = set_smem_optin((const void *)k_el_grad<true>, line_pass_smem(fft_len(h.plan[0]), h.L_line[0]));
   size_t m = 0;
-  for (int a = 1; a < h.ndim; ++a) m = std::max(m, line_pass_smem(h.N[a], h.L_line[a]));
+  for (int a = 1; a < h.ndim; ++a) m = std::max(m, line_pass_smem(fft_len(h.plan[a]), h.L_line[a]));
   if (e == cudaSuccess) e = set_smem_optin((const void *)k_el_grad<false>, m);
   for (int a = 0; a < h.ndim && e == cudaSuccess; ++a)
     if (el_fast(h, a)) e = fast_prime(h.N[a]);
@@ -398,7 +398,7 @@ cudaError_t el_prime(const SimDev &h) {
 cudaError_t el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
   if (el_fast(h, axis)) return fast_el_grad(h, axis, g, s, st);
   const int L = h.L_line[axis];
-  const size_t sm = line_pass_smem(h.N[axis], L);
+  const size_t sm = line_pass_smem(fft_len(h.plan[axis]), L);
   const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * L) * h.N[2]
                                     : (long long)cdiv(h.N[0], 2 * L) * (axis == 1 ? h.N[2] : h.N[1]);
   const int threads = pass_threads(h, tiles, (long long)L * h.N[axis]);

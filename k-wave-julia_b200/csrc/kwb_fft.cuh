@@ -192,13 +192,11 @@ __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ X, flo
   }
 }
 
-// Transform L lines held in X (Y is scratch of the same size; line pitch LS >= line_pitch(N)).  Returns the buffer holding the
-// result (X or Y).  Caller must __syncthreads() before (X filled) -- this function syncs after
-// every stage, so the result is visible to all threads on return.
+// The Stockham stages of `plan` on L lines of fft_len(plan) points held in X (Y is scratch).
 template <bool INV>
-__device__ float2 *fft_lines(float2 *X, float2 *Y, int L, int LS, const FftPlan &plan,
-                             const float2 *tw) {
-  const int N = plan.n;
+__device__ float2 *stockham_lines(float2 *X, float2 *Y, int L, int LS, const FftPlan &plan,
+                                  const float2 *tw) {
+  const int N = fft_len(plan);
   int Ns = 1;
   for (int s = 0; s < plan.nstages; ++s) {
     const int R = plan.radix[s];
@@ -218,6 +216,58 @@ __device__ float2 *fft_lines(float2 *X, float2 *Y, int L, int LS, const FftPlan 
     Ns *= R;
   }
   return X;
+}
+
+// Bluestein's algorithm for the n-point DFT of L lines (n = plan.n, first n slots of each line
+// in X; X and Y hold plan.m slots per line): with w_j = exp(-i pi j^2/n),
+//   X_k = w_k sum_j (x_j w_j) conj(w_{k-j}),
+// a circular convolution of length m >= 2n - 1 done as FFT_m, a multiply by the transform of
+// the conjugate chirp (chirp_ft, scaled by 1/m), and an inverse FFT_m.  The inverse DFT is the
+// conjugate of the forward DFT of the conjugate input.  tw: the m-point twiddles.
+template <bool INV>
+__device__ float2 *bluestein_lines(float2 *X, float2 *Y, int L, int LS, const FftPlan &plan,
+                                   const float2 *tw) {
+  const int n = plan.n, m = plan.m;
+  const float2 *__restrict__ w = plan.chirp;
+  const float2 *__restrict__ B = plan.chirp_ft;
+  for (int e = threadIdx.x; e < L * m; e += blockDim.x) {
+    const int l = e / m, j = e - l * m;
+    float2 a = make_float2(0.f, 0.f);
+    if (j < n) {
+      float2 x = X[l * LS + j];
+      if (INV) x.y = -x.y;
+      a = cmul(x, w[j]);
+    }
+    Y[l * LS + j] = a;
+  }
+  __syncthreads();
+  float2 *R = stockham_lines<false>(Y, X, L, LS, plan, tw);
+  float2 *F = (R == Y) ? X : Y;
+  for (int e = threadIdx.x; e < L * m; e += blockDim.x) {
+    const int l = e / m, j = e - l * m;
+    R[l * LS + j] = cmul(R[l * LS + j], B[j]);
+  }
+  __syncthreads();
+  float2 *C = stockham_lines<true>(R, F, L, LS, plan, tw);
+  for (int e = threadIdx.x; e < L * n; e += blockDim.x) {
+    const int l = e / n, k = e - l * n;
+    float2 v = cmul(C[l * LS + k], w[k]);
+    if (INV) v.y = -v.y;
+    C[l * LS + k] = v;
+  }
+  __syncthreads();
+  return C;
+}
+
+// Transform L lines held in X (Y is scratch of the same size; line pitch
+// LS >= line_pitch(fft_len(plan))).  Returns the buffer holding the result (X or Y), the first
+// plan.n slots of each line in natural order.  Caller must __syncthreads() before (X filled) --
+// this function syncs after every stage, so the result is visible to all threads on return.
+template <bool INV>
+__device__ float2 *fft_lines(float2 *X, float2 *Y, int L, int LS, const FftPlan &plan,
+                             const float2 *tw) {
+  if (plan.m > 0) return bluestein_lines<INV>(X, Y, L, LS, plan, tw);
+  return stockham_lines<INV>(X, Y, L, LS, plan, tw);
 }
 
 }  // namespace kwb

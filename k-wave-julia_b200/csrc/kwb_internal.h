@@ -19,6 +19,7 @@
 #define KWB_THREADS 256
 #define KWB_PASS_THREADS_MAX 1024  // Stockham passes on grids with few tiles (pass_threads)
 #define KWB_MAX_N 4096
+#define KWB_BLUESTEIN_MAX_N 2048  // Bluestein inner length 4096 at most: one line fits shared memory
 #define KWB_CHUNK_STEPS 32  // time steps per replayed CUDA graph
 
 // Programmatic dependent launch between the kernels of a time step.  Each step kernel is
@@ -33,11 +34,20 @@
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); \
   } while (0)
 
+// Stockham plan of a line of n points.  A length with a prime factor above 7 is transformed by
+// Bluestein's algorithm (chirp z-transform): m > 0 is the power-of-two length of the inner
+// transforms (m >= 2n - 1), the stages are m's, chirp[j] = exp(-i pi j^2 / n) (j < n) and
+// chirp_ft = FFT_m(conj chirp, wrapped) / m; m == 0 for a direct transform.
 struct FftPlan {
   int n;
   int nstages;
   int radix[KWB_MAX_STAGES];
+  int m;
+  const float2 *chirp;
+  const float2 *chirp_ft;
 };
+// Length of the transforms a plan runs (the buffers and twiddle table of a line are this long).
+__host__ __device__ inline int fft_len(const FftPlan &p) { return p.m > 0 ? p.m : p.n; }
 
 // Pass slots of the FFT schedule: line passes per axis, the x equation-of-state passes, the
 // y/z spectrum passes.
@@ -128,8 +138,8 @@ struct SimDev {
   // nullptr otherwise
   const float *inv_r;
   // 3-D equation of state with the y/z transforms in one cluster pass per kx plane: the half
-  // spectrum is then [z][kx][y] and M is [kx][slot][j] (slot: register order of the pass's y
-  // transform, j: register order of its z transform; fast_plane_slots)
+  // spectrum is then [z][kx][y] and M is [kx][k_z][slot] (slot: register order of the pass's y
+  // transform, fast_plane_slot_ky)
   int plane;
   // the x line pass ends with the equation of state's x R2C (no separate EOS forward pass)
   int fuse_xeos;
@@ -218,6 +228,9 @@ bool make_plan(int N, FftPlan &pl);
 // The same stages in another order: 0 as make_plan (8s first, then 4 or 2, then 3, 5, 7),
 // 1 radix-4 stages instead of 8s, 2 the odd radices first.
 bool make_plan_order(int N, FftPlan &pl, int order);
+// The plan of a line of N points: direct Stockham stages when N is 2/3/5/7-smooth, else
+// Bluestein with a power-of-two inner length (N <= KWB_BLUESTEIN_MAX_N); keeps pl's chirp tables.
+bool plan_line(int N, FftPlan &pl, int order);
 int choose_L(int N, int want, int cap_lines, int dispersion, bool spec);
 size_t line_pass_smem(int N, int L);
 size_t spec_pass_smem(int N, int L, int dispersion);
@@ -239,8 +252,18 @@ cudaError_t launch_advance_t0(long long *t0, long long k, cudaStream_t st);
 // Raise the dynamic shared-memory limit of every time-step kernel for this simulation's tiles.
 cudaError_t prime_attributes(const SimDev &h);
 
-// Register-FFT kernels (kwb_fast.cu) for line lengths 64, 128, 256, 512, 1024.
+// Register-FFT kernels (kwb_fast.cu) for line lengths 64, 128, 256, 512, 1024, and (through
+// kwb_fast_mixed.cu) the mixed-radix lengths 96, 160, 192, 320.
+struct ElGrad;
 bool fast_size(int N);
+bool fast_mixed_size(int N);
+cudaError_t fast_mixed_prime(int N);
+cudaError_t fast_mixed_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                                 cudaStream_t st);
+cudaError_t fast_mixed_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
+cudaError_t fast_mixed_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                            cudaStream_t st);
+cudaError_t fast_mixed_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
 cudaError_t fast_prime(int N);
 cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
                            cudaStream_t st);
@@ -249,8 +272,7 @@ cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, lo
                       cudaStream_t st);
 bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
-// Multiplier layout of the plane pass: Ny slot -> k_y entries, then Nz position -> k_z entries.
-void fast_plane_slots(int Ny, int Nz, int *tab);
+void fast_plane_slot_ky(int Ny, int *ky);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
 
 // Elastic solver kernels (kwb_elastic.cu).  One gradient pass along `axis` transforms up to

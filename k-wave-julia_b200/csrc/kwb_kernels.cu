@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(KWB_PASS_THREADS_MAX)
 
   const int N = S.N[axis];
   const int L = S.L_line[axis];
-  const int LS = line_pitch(N);
+  const int LS = line_pitch(fft_len(S.plan[axis]));
   const int Nx = S.N[0];
   float2 *X = smem;
   float2 *Y = X + L * LS;
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(KWB_PASS_THREADS_MAX)
     }
   };
   const int total = L * N;
-  load_twiddles(tw, S.tw[axis], N);
+  load_twiddles(tw, S.tw[axis], fft_len(S.plan[axis]));
   {
     const float *__restrict__ p = S.p;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   if (t >= S.Nt) return;
   const int N = S.N[0];
   const int L = S.L_eosx;
-  const int LS = line_pitch(N);
+  const int LS = line_pitch(fft_len(S.plan[0]));
   const int two = S.dispersion;
   const int LL = two ? 2 * L : L;
   float2 *X = smem;
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   float2 *tw = Y + LL * LS;
   const Tile T = tile_x(S, 2 * L, blockIdx.x);
   const int total = L * N;
-  load_twiddles(tw, S.tw[0], N);
+  load_twiddles(tw, S.tw[0], fft_len(S.plan[0]));
   const float inv_dt = 1.0f / S.dt;
   for (int e = threadIdx.x; e < total; e += blockDim.x) {
     const int l = e / N, i = e - l * N;
@@ -321,14 +321,14 @@ __global__ void __launch_bounds__(KWB_THREADS)
   if (t >= S.Nt) return;
   const int N = S.N[0];
   const int L = S.L_eosx;
-  const int LS = line_pitch(N);
+  const int LS = line_pitch(fft_len(S.plan[0]));
   float2 *X = smem;
   float2 *Y = X + L * LS;
   float2 *tw = Y + L * LS;
   const Tile T = tile_x(S, 2 * L, blockIdx.x);
   const int n1 = S.n1;
   const int Ny = S.N[1];
-  load_twiddles(tw, S.tw[0], N);
+  load_twiddles(tw, S.tw[0], fft_len(S.plan[0]));
   const bool even = (N & 1) == 0;
   for (int e = threadIdx.x; e < L * n1; e += blockDim.x) {
     const int l = e / n1, k = e - l * n1;
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
   if (t >= S.Nt) return;
   const int N = S.N[axis];
   const int L = S.L_spec[axis];
-  const int LS = line_pitch(N);
+  const int LS = line_pitch(fft_len(S.plan[axis]));
   const int two = S.dispersion && op != KWB_SPEC_INV;
   const int LL = two ? 2 * L : L;
   float2 *X = smem;
@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(KWB_THREADS)
     base = (long long)o * n1 + k0;
     stride = (long long)n1 * Ny;
   }
-  load_twiddles(tw, S.tw[axis], N);
+  load_twiddles(tw, S.tw[axis], fft_len(S.plan[axis]));
   const int total = L * N;
   for (int e = threadIdx.x; e < total; e += blockDim.x) {
     const int i = e / L, l = e - i * L;
@@ -557,7 +557,7 @@ cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int
                              long long step_s, cudaStream_t st) {
   if ((h.fast & 1) && fast_size(h.N[axis]) && (axis == 0 || h.N[0] % 4 == 0)) return fast_line_pass(d_sim, h, axis, mode, step_s, st);
   const int L = h.L_line[axis];
-  const size_t sm = line_pass_smem(h.N[axis], L);
+  const size_t sm = line_pass_smem(fft_len(h.plan[axis]), L);
   int tiles;
   if (axis == 0) {
     tiles = cdiv(h.N[1], 2 * L) * h.N[2];
@@ -574,7 +574,7 @@ cudaError_t launch_eos_x_fwd(const SimDev *d_sim, const SimDev &h, long long ste
                              cudaStream_t st) {
   if ((h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0])) return fast_eos(d_sim, h, true, step_s, st);
   const int L = h.L_eosx;
-  const size_t sm = spec_pass_smem(h.N[0], L, h.dispersion);
+  const size_t sm = spec_pass_smem(fft_len(h.plan[0]), L, h.dispersion);
   const int tiles = cdiv(h.N[1], 2 * L) * h.N[2];
   kwb_launch(k_eos_x_fwd, tiles, KWB_THREADS, sm, st, d_sim, step_s);
   return cudaGetLastError();
@@ -584,7 +584,7 @@ cudaError_t launch_eos_x_inv(const SimDev *d_sim, const SimDev &h, long long ste
                              cudaStream_t st) {
   if ((h.fast & 2) && h.ndim >= 2 && !h.dispersion && fast_size(h.N[0])) return fast_eos(d_sim, h, false, step_s, st);
   const int L = h.L_eosx;
-  const size_t sm = line_pass_smem(h.N[0], L);
+  const size_t sm = line_pass_smem(fft_len(h.plan[0]), L);
   const int tiles = cdiv(h.N[1], 2 * L) * h.N[2];
   kwb_launch(k_eos_x_inv, tiles, KWB_THREADS, sm, st, d_sim, step_s, h.ndim == 1 ? 1 : 0);
   return cudaGetLastError();
@@ -594,7 +594,7 @@ cudaError_t launch_spec_pass(const SimDev *d_sim, const SimDev &h, int axis, int
                              long long step_s, cudaStream_t st) {
   if ((h.fast & 2) && !h.dispersion && fast_size(h.N[axis])) return fast_spec(d_sim, h, axis, op, step_s, st);
   const int L = h.L_spec[axis];
-  const size_t sm = spec_pass_smem(h.N[axis], L, h.dispersion && op != KWB_SPEC_INV);
+  const size_t sm = spec_pass_smem(fft_len(h.plan[axis]), L, h.dispersion && op != KWB_SPEC_INV);
   const int tiles = cdiv(h.n1, L) * (axis == 1 ? h.N[2] : h.N[1]);
   kwb_launch(k_spec_pass, tiles, KWB_THREADS, sm, st, d_sim, axis, op, step_s);
   return cudaGetLastError();
@@ -618,13 +618,13 @@ cudaError_t launch_sensor_gather(const SimDev *d_sim, const SimDev &h, const Gro
 cudaError_t prime_attributes(const SimDev &h) {
   cudaError_t e;
   size_t m = 0;
-  if ((e = set_smem((const void *)k_line_pass<true>, line_pass_smem(h.N[0], h.L_line[0]))) != cudaSuccess) return e;
-  for (int a = 1; a < h.ndim; ++a) m = std::max(m, line_pass_smem(h.N[a], h.L_line[a]));
+  if ((e = set_smem((const void *)k_line_pass<true>, line_pass_smem(fft_len(h.plan[0]), h.L_line[0]))) != cudaSuccess) return e;
+  for (int a = 1; a < h.ndim; ++a) m = std::max(m, line_pass_smem(fft_len(h.plan[a]), h.L_line[a]));
   if ((e = set_smem((const void *)k_line_pass<false>, m)) != cudaSuccess) return e;
-  if ((e = set_smem((const void *)k_eos_x_fwd, spec_pass_smem(h.N[0], h.L_eosx, h.dispersion))) != cudaSuccess) return e;
-  if ((e = set_smem((const void *)k_eos_x_inv, line_pass_smem(h.N[0], h.L_eosx))) != cudaSuccess) return e;
+  if ((e = set_smem((const void *)k_eos_x_fwd, spec_pass_smem(fft_len(h.plan[0]), h.L_eosx, h.dispersion))) != cudaSuccess) return e;
+  if ((e = set_smem((const void *)k_eos_x_inv, line_pass_smem(fft_len(h.plan[0]), h.L_eosx))) != cudaSuccess) return e;
   m = 0;
-  for (int a = 1; a < h.ndim; ++a) m = std::max(m, spec_pass_smem(h.N[a], h.L_spec[a], h.dispersion));
+  for (int a = 1; a < h.ndim; ++a) m = std::max(m, spec_pass_smem(fft_len(h.plan[a]), h.L_spec[a], h.dispersion));
   if ((e = set_smem((const void *)k_spec_pass, m)) != cudaSuccess) return e;
   if (h.fast)
     for (int a = 0; a < h.ndim; ++a)

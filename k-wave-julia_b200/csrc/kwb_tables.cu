@@ -54,7 +54,7 @@ __global__ void k_build_pml_deficit(float *out, int N, int pml_size, double alph
 }
 
 // Layouts: [k_z][k_y][k_x] (slot_ky == nullptr) or, for the cluster plane pass,
-// [k_x][slot][j] with k_y = slot_ky[slot] and k_z = slot_ky[Ny + j].
+// [k_x][k_z][slot] with k_y = slot_ky[slot].
 __global__ void k_build_eos_multiplier(float *M, float *M2, int Nx, int Ny, int Nz, double dx,
                                        double dy, double dz, double c_ref, double dt,
                                        double c_sq_fold, int absorbing, double tau, double eta,
@@ -65,8 +65,8 @@ __global__ void k_build_eos_multiplier(float *M, float *M2, int Nx, int Ny, int 
   if (idx >= total) return;
   int kx, ky, kz;
   if (slot_ky) {
-    kz = slot_ky[Ny + (int)(idx % Nz)];
-    ky = slot_ky[(int)((idx / Nz) % Ny)];
+    ky = slot_ky[(int)(idx % Ny)];
+    kz = (int)((idx / Ny) % Nz);
     kx = (int)(idx / ((long long)Ny * Nz));
   } else {
     kx = (int)(idx % n1);

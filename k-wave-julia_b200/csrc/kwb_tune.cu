@@ -44,7 +44,7 @@ void schedule_apply(SimDev &h, const Schedule &s) {
     h.L_line[a] = s.L_line[a];
     h.L_spec[a] = s.L_spec[a];
     h.plan_order[a] = s.plan_order[a];
-    make_plan_order(h.N[a], h.plan[a], h.plan_order[a]);
+    plan_line(h.N[a], h.plan[a], h.plan_order[a]);
   }
   h.L_eosx = s.L_eosx;
 }
@@ -202,8 +202,8 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
     std::vector<int> orders;
     std::vector<FftPlan> plans;
     for (int o = 0; o < (explore_order ? 3 : 1); ++o) {
-      FftPlan pl;
-      if (!make_plan_order(t.N[a], pl, o)) continue;
+      FftPlan pl = t.plan[a];
+      if (!plan_line(t.N[a], pl, o)) continue;
       bool dup = false;
       for (const FftPlan &q : plans) dup |= q.nstages == pl.nstages && !memcmp(q.radix, pl.radix, pl.nstages * sizeof(int));
       if (dup) continue;
@@ -215,7 +215,7 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
       t.plan[a] = plans[i];
     }, go);
     const int cap = a == 0 ? (t.N[1] + 1) / 2 : (t.N[0] + 1) / 2;
-    const std::vector<int> Ls = l_candidates(t.N[a], t.L_line[a], cap, 0, false);
+    const std::vector<int> Ls = l_candidates(fft_len(t.plan[a]), t.L_line[a], cap, 0, false);
     T.choose("line_L", (int)Ls.size(), [&, a](int i) { t.L_line[a] = Ls[i]; }, go);
     const int thr[4] = {0, 256, 512, 1024};
     T.choose("line_threads", 4, [&, a](int i) { t.thr_line[a] = (short)thr[i]; }, go);
@@ -230,7 +230,7 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
       T.choose("eos_inv_tile", 3, [&](int i) { t.tile_var[KWB_SLOT_EOS_INV] = (signed char)i; },
                [&] { return launch_eos_x_inv(d, t, 0, st); });
     } else {
-      const std::vector<int> Ls = l_candidates(t.N[0], t.L_eosx, (t.N[1] + 1) / 2, t.dispersion, true);
+      const std::vector<int> Ls = l_candidates(fft_len(t.plan[0]), t.L_eosx, (t.N[1] + 1) / 2, t.dispersion, true);
       T.choose("eos_L", (int)Ls.size(), [&](int i) { t.L_eosx = Ls[i]; }, [&] {
         cudaError_t r = launch_eos_x_fwd(d, t, 0, st);
         return r == cudaSuccess ? launch_eos_x_inv(d, t, 0, st) : r;
@@ -245,7 +245,7 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
       if (spec_is_fast(t, a)) {
         T.choose("spec_tile", 3, [&, a](int i) { t.tile_var[KWB_SLOT_SPEC1 + a - 1] = (signed char)i; }, go);
       } else {
-        const std::vector<int> Ls = l_candidates(t.N[a], t.L_spec[a], t.n1, t.dispersion, true);
+        const std::vector<int> Ls = l_candidates(fft_len(t.plan[a]), t.L_spec[a], t.n1, t.dispersion, true);
         T.choose("spec_L", (int)Ls.size(), [&, a](int i) { t.L_spec[a] = Ls[i]; }, go);
       }
     }

@@ -359,8 +359,17 @@ def test_progress_callback_sees_every_step(kb):
     assert np.allclose([s[2] for s in seen], out["p"][lin, :], rtol=0, atol=1e-6)
 
 
+@pytest.mark.parametrize("shape", [(22, 16), (16, 22), (26, 20, 33), (44, 62)])
+def test_bluestein_lengths(kb, shape):
+    """Sides with a prime factor above 7 (22 = 2*11, 26 = 2*13, 33 = 3*11, 62 = 2*31) run through
+    Bluestein's algorithm on the Stockham kernels: parity with the oracle's FFTs of any length
+    (the reference's FFTW plans any N, fft_utils.jl:44-62)."""
+    case = _p0_case(shape, sum(shape), Nt=60, pml=4)
+    assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
+
+
 def test_errors_are_reported(kb):
-    n = 22  # 22 = 2 * 11: prime factor above 7
+    n = 2 * 1031  # 2 * 1031: prime factor above 7 and longer than the Bluestein limit (2048)
     g = kb.KWaveGrid(n, 1e-4, 16, 1e-4)
     kb.make_time(g, 1500.0, t_end=1e-6)
     with pytest.raises(kb.KWaveB200Error) as e:
@@ -403,10 +412,12 @@ def _p0_case(shape, seed, Nt, pml=8, record=("p_final", "p_max", "p_rms")):
 
 
 @pytest.mark.parametrize("shape", [(1024, 64), (64, 1024), (512, 128), (128, 512), (64, 64, 64), (32, 256, 32),
-                                   (64, 256, 256)])
+                                   (64, 256, 256), (192, 96), (96, 192), (160, 320), (320, 160), (96, 96, 96),
+                                   (192, 64, 160), (64, 320, 192)])
 def test_register_fft_sizes(kb, shape):
-    """Every register-FFT line length (64..1024) on both the contiguous x axis and strided axes;
-    (64, 256, 256) takes the cluster plane pass for the y/z spectrum transforms."""
+    """Every register-FFT line length (64..1024 and the mixed-radix 96, 160, 192, 320) on both the
+    contiguous x axis and strided axes; (64, 256, 256) takes the cluster plane pass for the y/z
+    spectrum transforms."""
     case = _p0_case(shape, sum(shape), Nt=60)
     assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
 
