@@ -518,6 +518,173 @@ struct LineFFT3G {
   }
 };
 
+// Four levels for longer mixed-radix lines: N = R1 * A * B * C with A, B, C powers of two
+// dividing R1 (384 = 12*4*4*2, 768 = 12*4*4*4), G = A*B*C threads per line.  The G-point DFT
+// over u = a + A (b + B c) is split three ways (m = m_c + C (m_b + B m_a)):
+//   Y[m] = sum_a w_A^{a m_a} w_G^{a (m_c + C m_b)} sum_b w_B^{b m_b} w_BC^{b m_c} sum_c w_C^{c m_c} y[u],
+// so after the R1-point register DFT and its twiddles, level 2 takes C-point DFTs over c (twiddle
+// w_BC^{b m_c}), level 3 B-point DFTs over b (twiddle w_G^{a (m_c + C m_b)}) and level 4
+// A-point DFTs over a; thread t then holds X[q1 + R1 (m_c + C (m_b + B m_a))].  Exchanges use
+// generic odd pitches.
+template <int R1, int A, int B, int C, bool WARP>
+struct LineFFT4G {
+  static constexpr int E = R1, G = A * B * C, N = R1 * A * B * C;
+  static constexpr int P2 = R1 / C, P3 = R1 / B, P4 = R1 / A;
+  static_assert(R1 % A == 0 && R1 % B == 0 && R1 % C == 0, "LineFFT4G shape");
+  static constexpr int RP = G + 1;  // level-1 twiddle pitch and exchange pitch
+  // exchange layouts: level 1 [q][u]; level 2 [q1][a][m_c][b]; level 3 [q1][m_b][m_c][a]
+  static constexpr int Q2 = A * (C * (B + 1)) + 1, Q3 = B * (C * (A + 1)) + 1;
+  __host__ __device__ static constexpr int nat(int k) { return k + (k >> 5); }
+  __device__ __forceinline__ static int i1(int q, int u) { return q * RP + u; }
+  __device__ __forceinline__ static int i2(int q1, int a, int mc, int b) { return q1 * Q2 + (a * C + mc) * (B + 1) + b; }
+  __device__ __forceinline__ static int i3(int q1, int mb, int mc, int a) { return q1 * Q3 + (mb * C + mc) * (A + 1) + a; }
+  static constexpr int S1 = (R1 - 1) * RP + G, S2 = R1 * Q2, S3 = R1 * Q3, S4 = N + (N >> 5);
+  static constexpr int SA = S1 > S2 ? S1 : S2, SB = S3 > S4 ? S3 : S4, SM = SA > SB ? SA : SB;
+  static constexpr int LP = SM | 1;
+  // twiddles: level 1 exp(-2 pi i u q/N) [q][u]; level 2 w_BC^{b m_c} [m_c][b];
+  // level 3 w_G^{a (m_c + C m_b)} [m_b][m_c][a]
+  static constexpr int T2 = R1 * RP, T3 = T2 + C * (B + 1);
+  static constexpr int TW = T3 + B * C * (A + 1);
+  static constexpr bool WARP_SYNC = WARP;
+  __device__ __forceinline__ static void sync() {
+    if (WARP) __syncwarp();
+    else __syncthreads();
+  }
+  // level-4 work item p = t P4 + j -> (q1, m_b, m_c) = p in [R1][B][C] order
+  __host__ __device__ __forceinline__ static int k_of(int t, int idx) {
+    const int p = t * P4 + idx / A, q1 = p / (B * C), r = p - q1 * B * C, mb = r / C, mc = r - mb * C;
+    return q1 + R1 * (mc + C * (mb + B * (idx % A)));
+  }
+  __device__ __forceinline__ static int nat_of(int t, int idx) { return nat(k_of(t, idx)); }
+  __device__ __forceinline__ static void build_tw(float2 *tw, const float2 *g) {
+    for (int e = threadIdx.x; e < R1 * G; e += blockDim.x) {
+      const int q = e / G, u = e - q * G;
+      tw[q * RP + u] = g[u * q];
+    }
+    constexpr int NG = N / G;  // g[j NG] = exp(-2 pi i j/G)
+    for (int e = threadIdx.x; e < C * B; e += blockDim.x) {
+      const int mc = e / B, b = e - mc * B;
+      tw[T2 + mc * (B + 1) + b] = g[NG * A * b * mc];  // w_BC^{b m_c} = w_G^{A b m_c}
+    }
+    for (int e = threadIdx.x; e < B * C * A; e += blockDim.x) {
+      const int mb = e / (C * A), r = e - mb * C * A, mc = r / A, a = r - mc * A;
+      tw[T3 + (mb * C + mc) * (A + 1) + a] = g[NG * ((a * (mc + C * mb)) % G)];
+    }
+  }
+  __device__ __forceinline__ static void fwd(float2 (&v)[E], float2 *xs, const float2 *tw, int t) {
+    dft_mixed<R1, false>(v);
+#pragma unroll
+    for (int q = 0; q < R1; ++q) xs[i1(q, t)] = q == 0 ? v[q] : cmul(v[q], tw[q * RP + t]);
+    sync();
+    // level 2: (q1, a, b) = t P2 + j in [R1][A][B] order; C-point DFT over c
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / (A * B), r = p - q1 * A * B, a = r / B, b = r - a * B;
+      float2 w[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) w[c] = xs[i1(q1, a + A * (b + B * c))];
+      dft_reg<C, false>(w);
+#pragma unroll
+      for (int mc = 0; mc < C; ++mc) v[j * C + mc] = (mc == 0 || b == 0) ? w[mc] : cmul(w[mc], tw[T2 + mc * (B + 1) + b]);
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / (A * B), r = p - q1 * A * B, a = r / B, b = r - a * B;
+#pragma unroll
+      for (int mc = 0; mc < C; ++mc) xs[i2(q1, a, mc, b)] = v[j * C + mc];
+    }
+    sync();
+    // level 3: (q1, a, m_c) = t P3 + j in [R1][A][C] order; B-point DFT over b
+#pragma unroll
+    for (int j = 0; j < P3; ++j) {
+      const int p = t * P3 + j, q1 = p / (A * C), r = p - q1 * A * C, a = r / C, mc = r - a * C;
+      float2 w[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) w[b] = xs[i2(q1, a, mc, b)];
+      dft_reg<B, false>(w);
+#pragma unroll
+      for (int mb = 0; mb < B; ++mb) v[j * B + mb] = a == 0 ? w[mb] : cmul(w[mb], tw[T3 + (mb * C + mc) * (A + 1) + a]);
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P3; ++j) {
+      const int p = t * P3 + j, q1 = p / (A * C), r = p - q1 * A * C, a = r / C, mc = r - a * C;
+#pragma unroll
+      for (int mb = 0; mb < B; ++mb) xs[i3(q1, mb, mc, a)] = v[j * B + mb];
+    }
+    sync();
+    // level 4: (q1, m_b, m_c) = t P4 + j in [R1][B][C] order; A-point DFT over a
+#pragma unroll
+    for (int j = 0; j < P4; ++j) {
+      const int p = t * P4 + j, q1 = p / (B * C), r = p - q1 * B * C, mb = r / C, mc = r - mb * C;
+      float2 w[A];
+#pragma unroll
+      for (int a = 0; a < A; ++a) w[a] = xs[i3(q1, mb, mc, a)];
+      dft_reg<A, false>(w);
+#pragma unroll
+      for (int ma = 0; ma < A; ++ma) v[j * A + ma] = w[ma];
+    }
+    sync();
+  }
+  // exact reverse of fwd with conjugate twiddles (unnormalised); out: v[r] = x[t + G r]
+  __device__ __forceinline__ static void inv(float2 (&v)[E], float2 *xs, const float2 *tw, int t) {
+#pragma unroll
+    for (int j = 0; j < P4; ++j) {
+      const int p = t * P4 + j, q1 = p / (B * C), r = p - q1 * B * C, mb = r / C, mc = r - mb * C;
+      float2 w[A];
+#pragma unroll
+      for (int ma = 0; ma < A; ++ma) w[ma] = v[j * A + ma];
+      dft_reg<A, true>(w);
+#pragma unroll
+      for (int a = 0; a < A; ++a) xs[i3(q1, mb, mc, a)] = w[a];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P3; ++j) {
+      const int p = t * P3 + j, q1 = p / (A * C), r = p - q1 * A * C, a = r / C, mc = r - a * C;
+      float2 w[B];
+#pragma unroll
+      for (int mb = 0; mb < B; ++mb)
+        w[mb] = a == 0 ? xs[i3(q1, mb, mc, a)] : cmul_conj(xs[i3(q1, mb, mc, a)], tw[T3 + (mb * C + mc) * (A + 1) + a]);
+      dft_reg<B, true>(w);
+#pragma unroll
+      for (int b = 0; b < B; ++b) v[j * B + b] = w[b];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P3; ++j) {
+      const int p = t * P3 + j, q1 = p / (A * C), r = p - q1 * A * C, a = r / C, mc = r - a * C;
+#pragma unroll
+      for (int b = 0; b < B; ++b) xs[i2(q1, a, mc, b)] = v[j * B + b];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / (A * B), r = p - q1 * A * B, a = r / B, b = r - a * B;
+      float2 w[C];
+#pragma unroll
+      for (int mc = 0; mc < C; ++mc)
+        w[mc] = (mc == 0 || b == 0) ? xs[i2(q1, a, mc, b)] : cmul_conj(xs[i2(q1, a, mc, b)], tw[T2 + mc * (B + 1) + b]);
+      dft_reg<C, true>(w);
+#pragma unroll
+      for (int c = 0; c < C; ++c) v[j * C + c] = w[c];
+    }
+    sync();
+#pragma unroll
+    for (int j = 0; j < P2; ++j) {
+      const int p = t * P2 + j, q1 = p / (A * B), r = p - q1 * A * B, a = r / B, b = r - a * B;
+#pragma unroll
+      for (int c = 0; c < C; ++c) xs[i1(q1, a + A * (b + B * c))] = v[j * C + c];
+    }
+    sync();
+#pragma unroll
+    for (int q = 0; q < R1; ++q) v[q] = q == 0 ? xs[i1(q, t)] : cmul_conj(xs[i1(q, t)], tw[q * RP + t]);
+    dft_mixed<R1, true>(v);
+    sync();
+  }
+};
+
 // Build the per-CTA tables: tw2 (and, for line passes, the gradient multipliers in register order).
 template <int E, int G>
 __device__ __forceinline__ void build_tables(float2 *tw2, float2 *gp2, float2 *gn2, const float2 *tw,
@@ -1448,6 +1615,17 @@ struct LinePolicy<192> {
 template <>
 struct LinePolicy<320> {
   template <bool C> using F = LineFFT3G<20, 4, 4, C>;
+  static constexpr int THREADS = 256, MINB = 2;
+};
+
+template <>
+struct LinePolicy<384> {
+  template <bool C> using F = LineFFT4G<12, 4, 4, 2, C>;
+  static constexpr int THREADS = 256, MINB = 2;
+};
+template <>
+struct LinePolicy<768> {
+  template <bool C> using F = LineFFT4G<12, 4, 4, 4, false>;  // 64 threads per line: block-level sync
   static constexpr int THREADS = 256, MINB = 2;
 };
 

@@ -51,3 +51,19 @@ def test_c2_full_horizon_against_fp64_golden(wl):
         rep[k] = (l2, mx)
         assert l2 <= TOL_L2 and mx <= TOL_MAX, (k, l2, mx)
     print("c2 512^2 x 2000", rep)
+
+
+def test_sampled_serving_requests_against_fp64_golden(wl):
+    """Requests 0, 16 and 22 of the 48-request serving stream (two 2D, one 64^3), served together
+    through the continuous-batching scheduler: each p series against the FP64 oracle's
+    (tests/golden/serving_sample.npz)."""
+    import kwave_b200 as kb
+    gold = np.load(os.path.join(GOLDEN, "serving_sample.npz"))
+    reqs = {}
+    for i in gold["requests"]:
+        case = wl.c5_request(int(i), seed=5005, nt_range=(300, 800))
+        g, m, s, sen, kw = case.to_api()
+        reqs[int(i)] = kb.submit(g, m, s, sen, **kw)
+    for i, r in reqs.items():
+        l2, mx = errors(r.result()["p"], gold[f"p_{i}"].astype(np.float64))
+        assert l2 <= TOL_L2 and mx <= TOL_MAX, (i, l2, mx)
