@@ -1049,6 +1049,12 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   }
 
   // ---- fields
+  CU(M.alloc(&h.err, 1));
+  CU(cudaMemsetAsync(h.err, 0, sizeof(int), st));
+  {
+    const char *dc = getenv("KWB_TEST_DROP_TILE_COPY");
+    h.test_drop_copy = dc && strcmp(dc, "1") == 0;
+  }
   CU(M.alloc(&h.p, nvox));
   CU(cudaMemsetAsync(h.p, 0, nvox * 4, st));
   for (int d = 0; d < D; ++d) {
@@ -1570,6 +1576,20 @@ int kwb_sim_advance(kwb_sim *S, int64_t steps) {
   return sim_enqueue(S, steps);
 }
 
+// The device error word: set by a kernel whose bounded wait gave up (a tile copy into shared
+// memory that did not complete in its time budget).  Read after the stream is synchronised.
+static int check_device_err(kwb_sim *S) {
+  if (!S->h.err) return KWB_OK;
+  kwb_ctx *ctx = S->ctx;
+  int e = 0;
+  CU(cudaMemcpy(&e, S->h.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e)
+    return set_err(ctx, KWB_E_DEVICE,
+                   "a device-side wait gave up: a tile copy into shared memory did not complete within "
+                   "its time budget (error word %d)", e);
+  return KWB_OK;
+}
+
 int kwb_sim_advance_timed(kwb_sim *S, int64_t steps, double *device_ms) {
   if (!S) return KWB_E_INVALID;
   kwb_ctx *ctx = S->ctx;
@@ -1587,7 +1607,7 @@ int kwb_sim_advance_timed(kwb_sim *S, int64_t steps, double *device_ms) {
   float ms = 0;
   CU(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
   if (device_ms) *device_ms = ms;
-  return KWB_OK;
+  return check_device_err(S);
 }
 
 int64_t kwb_sim_steps_done(const kwb_sim *S) { return S ? S->steps_done : -1; }
@@ -1596,7 +1616,7 @@ int kwb_sim_sync(kwb_sim *S) {
   if (!S) return KWB_E_INVALID;
   kwb_ctx *ctx = S->ctx;
   CU(cudaStreamSynchronize(S->stream));
-  return KWB_OK;
+  return check_device_err(S);
 }
 
 int kwb_sim_read_pressure(kwb_sim *S, float *p_host) {
@@ -1646,6 +1666,7 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
   kwb_ctx *ctx = S->ctx;
   CU(cudaSetDevice(ctx->device));
   CU(cudaStreamSynchronize(S->stream));
+  if (const int erc = check_device_err(S)) return erc;
   const double Ntd = (double)S->Nt_loop;
   for (size_t g = 0; g < S->groups.size(); ++g) {
     if (!out->groups) break;

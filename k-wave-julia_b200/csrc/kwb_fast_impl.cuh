@@ -748,6 +748,40 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Bulk (TMA) copies global -> shared completing on an mbarrier (no multicast).
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *m, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+// order this thread's earlier generic-proxy accesses of shared memory before async-proxy writes
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *m, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *m) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(m))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *m, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of an mbarrier, giving up after about 2^30 SM clocks (half a second):
+// false means the copies it tracks did not complete, which the caller reports instead of hanging.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *m, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(m, parity))
+    if (clock64() - t0 > (1LL << 30)) return false;
+  return true;
+}
+
 // ------------------------------------------------------------------------------------------
 // fused per-axis line pass (same algorithm as kwb::k_line_pass)
 // ------------------------------------------------------------------------------------------
@@ -766,11 +800,23 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   float2 *tw2 = sm + L * LP;
   float2 *gp2 = tw2 + F::TW;
   float2 *gn2 = gp2 + E * RP;
+  // Contiguous tiles are 2L whole consecutive rows, so each field's tile is one block of
+  // memory: one bulk (TMA) copy per field, completing on its own mbarrier (0 p, 1 rho0,
+  // 2 u_d, 3 rho_d; each used for one phase).
+  __shared__ __align__(8) unsigned long long tile_bar[4];
+  if (CONTIG && threadIdx.x == 0) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) mbar_init(&tile_bar[b], 1);
+  }
   // the tables are written once at set-up: built before waiting on the previous kernel
   build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
+  if (CONTIG) __syncthreads();  // the mbarriers are initialised for every thread
   KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (mode == KWB_MODE_STEP && t >= S.Nt) return;
+  // once a wait has given up, the simulation is failed: later tiles exit at once instead of each
+  // waiting out its budget (uniform over the CTA: one load before any thread diverges)
+  if (CONTIG && *reinterpret_cast<volatile const int *>(S.err) != 0) return;
   const int tid = threadIdx.x;
   const int tt = CONTIG ? tid % G : tid / L;
   const int l = CONTIG ? tid / G : tid % L;
@@ -830,16 +876,17 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   float *st_r = st_p + 2 * L * N;
   // Chunk assignments are compile-time strides from a per-thread start, so the addresses of a
   // thread's chunks differ by constants.
-  auto stage = [&](float *dst, const float *f) {
+  auto stage = [&](float *dst, const float *f, int slot) {
     const float *fb = f + base;
     if (CONTIG) {
-      constexpr int CH = 2 * L * N / 4, PER = (CH + THREADS - 1) / THREADS;  // rows contiguous in memory
-      const int chunks = cnt * N / 4;
-#pragma unroll
-      for (int k = 0; k < PER; ++k) {
-        const int q = tid + k * THREADS;
-        if (q < chunks) cp_async16(dst + 4 * q, fb + 4 * q, 16);
+      // rows contiguous in memory: one bulk copy of cnt rows (16-byte aligned: N % 4 == 0)
+      if (tid == 0) {
+        const unsigned bytes = (unsigned)cnt * N * 4u;
+        fence_proxy_async_smem();
+        mbar_expect_tx(&tile_bar[slot], bytes);
+        if (!(S.test_drop_copy && slot == 0 && blockIdx.x == 0)) bulk_copy_g2s(dst, fb, bytes, &tile_bar[slot]);
       }
+      return;
     } else {
       constexpr int CPR = (2 * L) / 4;  // 16-byte chunks per tile row (strided tiles have L >= 2)
       static_assert(THREADS % CPR == 0 && (CPR * N) % THREADS == 0, "strided staging");
@@ -855,18 +902,43 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     }
     cp_async_commit();
   };
+  // Contiguous tiles: wait (bounded) for the bulk copies of the given slots, uniformly over the
+  // CTA.  On a timeout the error word is set and the tile is abandoned: the remaining waits drain
+  // any copy still in flight before the CTA exits.
+  bool issued[4] = {false, false, false, false};
+  auto tile_wait = [&](int s0, int s1) -> bool {
+    bool ok = true;
+    if (s0 >= 0) ok = mbar_wait_bounded(&tile_bar[s0], 0) && ok;
+    if (s1 >= 0) ok = mbar_wait_bounded(&tile_bar[s1], 0) && ok;
+    ok = __syncthreads_and(ok);
+    if (!ok) {
+      if (tid == 0) atomicOr(S.err, 1);
+      for (int b = 0; b < 4; ++b)
+        if (issued[b]) mbar_wait_bounded(&tile_bar[b], 0);
+    }
+    return ok;
+  };
   auto staged = [&](const float *st, int i) -> float2 {
     if (CONTIG) return make_float2(va ? st[(2 * l) * N + i] : 0.f, vb ? st[(2 * l + 1) * N + i] : 0.f);
     return *reinterpret_cast<const float2 *>(st + i * 2 * L + 2 * l);
   };
   const float *__restrict__ rho0 = S.rho0;
-  stage(st_p, S.p);
-  if (rho0) stage(st_r, rho0);
-  else cp_async_commit();
+  stage(st_p, S.p, 0);
+  issued[0] = true;
+  if (rho0) {
+    stage(st_r, rho0, 1);
+    issued[1] = true;
+  } else if (!CONTIG) {
+    cp_async_commit();
+  }
   float2 *xs = sm + l * LP;
   float *__restrict__ ud = S.u[axis];
-  cp_async_wait<1>();  // the p tile has landed (rho0 may still be in flight)
-  __syncthreads();     // ... for every thread; tables too
+  if constexpr (CONTIG) {
+    if (!tile_wait(0, -1)) return;  // the p tile has landed (rho0 may still be in flight)
+  } else {
+    cp_async_wait<1>();  // the p tile has landed (rho0 may still be in flight)
+    __syncthreads();     // ... for every thread; tables too
+  }
   float2 v[E];
 #pragma unroll
   for (int r = 0; r < E; ++r) v[r] = staged(st_p, tt + G * r);
@@ -874,7 +946,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // (INIT keeps p staged: it is read again below)
   if (mode == KWB_MODE_STEP) {
     __syncthreads();  // every thread has its p values
-    stage(st_p, ud);
+    stage(st_p, ud, 2);
+    issued[2] = true;
   }
 
   // d/dx_d p  (staggered +)
@@ -882,8 +955,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gp2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
-  cp_async_wait<0>();
-  __syncthreads();  // the rho0 and velocity tiles have landed
+  if constexpr (CONTIG) {
+    if (!tile_wait(rho0 ? 1 : -1, mode == KWB_MODE_STEP ? 2 : -1)) return;
+  } else {
+    cp_async_wait<0>();
+    __syncthreads();  // the rho0 and velocity tiles have landed
+  }
 
   // velocity update u = pml_sg (pml_sg u - dt/rho_sg dp)
   const float *__restrict__ esg = S.pml_sg_def[axis];
@@ -927,7 +1004,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 
   // the split density rho_d takes the slot while d/dx_d u is transformed
   __syncthreads();  // every thread is done with the velocity tile
-  stage(st_p, S.rho[axis]);
+  stage(st_p, S.rho[axis], 3);
+  issued[3] = true;
 
   // velocity sources on this tile's lines (first_order_steps.jl:586-617, 646-690)
   // (entries are sorted by line: a thread scans only its own two lines)
@@ -959,8 +1037,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gn2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
 
-  cp_async_wait<0>();
-  __syncthreads();  // the rho_d tile has landed
+  if constexpr (CONTIG) {
+    if (!tile_wait(3, -1)) return;  // the rho_d tile has landed
+  } else {
+    cp_async_wait<0>();
+    __syncthreads();  // the rho_d tile has landed
+  }
   // density update rho_d = pml (pml rho_d - dt rho0 du)
   const float *__restrict__ ed = S.pml_def[axis];
 #pragma unroll
@@ -1882,6 +1964,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     }
     cp_async_commit();
   };
+
   auto staged = [&](const float *st, int i) -> float2 {
     if (CONTIG) return make_float2(va ? st[(2 * l) * N + i] : 0.f, vb ? st[(2 * l + 1) * N + i] : 0.f);
     return *reinterpret_cast<const float2 *>(st + i * 2 * L + 2 * l);

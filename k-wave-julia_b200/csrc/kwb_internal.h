@@ -151,6 +151,10 @@ struct SimDev {
   // GroupDev::line_ptr / line_ent); nullptr when there is none.
   const struct GroupDev *sparse_p;
 
+  // Device error word: kernels set bit 0 when a bounded wait gave up (a tile copy that did not
+  // complete); the host reads it after synchronising and reports KWB_E_DEVICE.
+  int *err;
+  int test_drop_copy;  // test hook: the first CTA of a contiguous line pass drops its p-tile copy
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
   // Measured FFT schedule (kwb_tune.cu): register-FFT tile variant per pass slot (KWB_SLOT_*;

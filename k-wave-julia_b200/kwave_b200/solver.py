@@ -629,6 +629,16 @@ class Request:
     def cancel(self):
         check(self.ctx.lib, self.ctx.handle, self.ctx.lib.kwb_cancel(self.ctx.handle, self.ticket))
 
+    def __del__(self):
+        # The scheduler reads this request's problem arrays and writes its output buffers until it
+        # completes: a request dropped unwaited is cancelled and waited for before they are freed.
+        try:
+            if self._result is None and self.info is None and getattr(self.ctx, "handle", None):
+                self.ctx.lib.kwb_cancel(self.ctx.handle, self.ticket)
+                self.ctx.lib.kwb_wait(self.ctx.handle, self.ticket, -1, None)
+        except Exception:
+            pass
+
     @property
     def latency_s(self) -> Optional[float]:
         return None if self.info is None else (self.info["end_ns"] - self.info["submit_ns"]) / 1e9

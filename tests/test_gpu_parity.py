@@ -368,6 +368,27 @@ def test_bluestein_lengths(kb, shape):
     assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
 
 
+def test_bounded_tile_wait_reports_an_error(kb, monkeypatch):
+    """The contiguous line pass stages its tiles with bulk (TMA) copies completing on mbarriers;
+    every wait is bounded by a clock budget.  With the test hook the first CTA's p-tile copy is
+    never issued, so its wait runs out (about half a second): the kernel sets the device error
+    word and returns, the host reports KWB_E_DEVICE, and the context keeps working."""
+    from kwave_b200.workloads import c2
+    monkeypatch.setenv("KWB_TUNE", "0")
+    monkeypatch.setenv("KWB_TEST_DROP_TILE_COPY", "1")
+    case = c2(n=256, Nt=4, record=("p_max",))
+    g, m, s, sen, kw = case.to_api()
+    sim = kb.Simulation(g, m, s, sen, **kw)
+    with pytest.raises(kb.KWaveB200Error) as e:
+        sim.advance(2)
+        sim.sync()
+    assert e.value.code == -4 and "gave up" in str(e.value)
+    sim.close()
+    monkeypatch.delenv("KWB_TEST_DROP_TILE_COPY")
+    ok = c2(n=256, Nt=30, record=("p_max", "p_rms"))
+    assert_parity(run_gpu(ok), run_oracle(ok), TOL_L2, TOL_MAX)
+
+
 def test_errors_are_reported(kb):
     n = 2 * 1031  # 2 * 1031: prime factor above 7 and longer than the Bluestein limit (2048)
     g = kb.KWaveGrid(n, 1e-4, 16, 1e-4)

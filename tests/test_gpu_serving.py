@@ -91,11 +91,12 @@ def test_cancel_and_failures_stay_per_request():
                         kb.estimate_device_bytes(gb, mb, sb, senb, context=ctx, **kwb)))
     kb.serving_config(max_running=4, chunk_steps=4, mem_cap_bytes=cap, context=ctx)
     # an invalid problem is rejected synchronously at submission, like the reference's error()
-    bad_g = kb.KWaveGrid(22, 1e-4, 16, 1e-4)  # 22 = 2 * 11: unsupported radix
+    nb = 2 * 1031  # a prime factor above 7 and longer than the Bluestein limit: unsupported
+    bad_g = kb.KWaveGrid(nb, 1e-4, 16, 1e-4)
     kb.make_time(bad_g, 1500.0, t_end=1e-6)
     with pytest.raises(kb.KWaveB200Error) as e:
-        kb.submit(bad_g, kb.KWaveMedium(sound_speed=1500.0), kb.KWaveSource(p0=np.ones((22, 16))),
-                  kb.KWaveSensor(mask=np.ones((22, 16), bool)), context=ctx)
+        kb.submit(bad_g, kb.KWaveMedium(sound_speed=1500.0), kb.KWaveSource(p0=np.ones((nb, 16))),
+                  kb.KWaveSensor(mask=np.ones((nb, 16), bool)), context=ctx)
     assert e.value.code == -2
     r_long = kb.submit(g, m, s, sen, context=ctx, **kw)
     g2, m2, s2, sen2, kw2 = big.to_api()
