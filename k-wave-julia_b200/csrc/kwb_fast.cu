@@ -12,14 +12,22 @@ bool fast_plane_available() {
   if (n < 0) n = fast::plane_clusters_per_device();
   return n > 0;
 }
+// Plane-pass variants usable on this device (1 or 2: the 16-CTA clusters need the non-portable
+// cluster size).
+int fast_plane_variants() {
+  static int v = -1;
+  if (v < 0) v = !fast_plane_available() ? 0 : (fast::plane_clusters_of<1>() > 0 ? 2 : 1);
+  return v;
+}
 // Register-order slot -> k_y of the plane pass's y transform (the layout of its multiplier).
 void fast_plane_slot_ky(int Ny, int *ky) {
   using F = fast::PlaneFY;
   for (int s = 0; s < Ny; ++s) ky[s] = F::k_of(s % F::G, s / F::G);
 }
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
-  kwb_launch(fast::k_plane_fast<fast::PlaneFY, fast::PlaneFZ, fast::kPlaneCL>, h.n1 * fast::kPlaneCL, KWB_PLANE_THREADS, fast::plane_smem(), st, h, s);
-  return cudaGetLastError();
+  (void)d_sim;
+  const int v = h.tile_var[KWB_SLOT_PLANE] == 1 && fast_plane_variants() > 1 ? 1 : 0;
+  return v == 1 ? fast::plane_launch<1>(h, s, st) : fast::plane_launch<0>(h, s, st);
 }
 
 bool fast_size(int N) { return N == 64 || N == 128 || N == 256 || N == 512 || N == 1024 || fast_mixed_size(N); }

@@ -1511,12 +1511,15 @@ __device__ __forceinline__ unsigned cluster_rank() {
 //      back, storing each element to the CTA it came from;
 //   3. after a second barrier, transforms its rows back along y and writes them to the plane.
 // The spectrum crosses HBM once in and once out per step, with the multiplier read once.
-template <class FY, class FZ, int CL>
-__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 2)
+// The cluster shape is set at launch (CL CTAs of THREADS threads: 8 x 512, or 16 x 256 with half
+// the rows per CTA so that four CTAs fit an SM); element z of a z line sits in row z % RZ of
+// cluster CTA z / RZ.
+template <class FY, class FZ, int CL, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
     k_plane_fast(const __grid_constant__ SimDev S, long long step_s) {
   constexpr int NY = FY::N, NZ = FZ::N, RZ = NZ / CL, CY = NY / CL;
-  constexpr int LY = KWB_PLANE_THREADS / FY::G, LZ = KWB_PLANE_THREADS / FZ::G;
-  static_assert(RZ == 2 * LY && CY % LZ == 0 && RZ == FZ::G, "plane tiling");
+  constexpr int LY = THREADS / FY::G, LZ = THREADS / FZ::G;
+  static_assert(RZ == 2 * LY && CY % LZ == 0 && NZ % RZ == 0, "plane tiling");
   constexpr int XS = (LY * FY::LP > LZ * FZ::LP) ? LY * FY::LP : LZ * FZ::LP;
   extern __shared__ float4 smem_raw[];
   float2 *data = reinterpret_cast<float2 *>(smem_raw);  // [RZ][NY]
@@ -1538,7 +1541,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 
   constexpr int CPR = NY / 2;  // 16-byte chunks per row
 #pragma unroll
   for (int g = 0; g < 2; ++g) {
-    for (int q = tid; q < LY * CPR; q += KWB_PLANE_THREADS) {
+    for (int q = tid; q < LY * CPR; q += THREADS) {
       const int r = g * LY + q / CPR, c = q % CPR;
       cp_async16(data + r * NY + 2 * c, plane + r * rstride + 2 * c, 16);
     }
@@ -1573,11 +1576,13 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 
 #pragma unroll 1
     for (int c0 = 0; c0 < CY; c0 += LZ) {
       const int sl = (int)rank * CY + c0 + l;  // slot (register-order k_y) of this line
-      // element z = tt + G r is row tt of CTA r (RZ == G)
-      const unsigned a0 = cta_smem_addr(data + tt * NY + sl);
+      // element z = tt + G r is row z % RZ of CTA z / RZ
       float2 v[FZ::E];
 #pragma unroll
-      for (int r = 0; r < FZ::E; ++r) v[r] = cluster_ld(cluster_map(a0, (unsigned)r));
+      for (int r = 0; r < FZ::E; ++r) {
+        const int z = tt + FZ::G * r;
+        v[r] = cluster_ld(cluster_map(cta_smem_addr(data + (z % RZ) * NY + sl), (unsigned)(z / RZ)));
+      }
       FZ::fwd(v, xs, twz, tt);
       // the multiplier is loaded after the transform: held across it, it spilled
 #pragma unroll
@@ -1587,7 +1592,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(KWB_PLANE_THREADS, 
       }
       FZ::inv(v, xs, twz, tt);
 #pragma unroll
-      for (int r = 0; r < FZ::E; ++r) cluster_st(cluster_map(a0, (unsigned)r), v[r]);
+      for (int r = 0; r < FZ::E; ++r) {
+        const int z = tt + FZ::G * r;
+        cluster_st(cluster_map(cta_smem_addr(data + (z % RZ) * NY + sl), (unsigned)(z / RZ)), v[r]);
+      }
     }
   }
   cluster_barrier();
@@ -1856,35 +1864,72 @@ static inline cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, in
   return cudaGetLastError();
 }
 
-// Cluster plane pass for Ny = Nz = 256: 8 CTAs of 512 threads per kx plane, 32 rows each.
+// Cluster plane pass for Ny = Nz = 256: variant 0 has 8 CTAs of 512 threads per kx plane (32 rows
+// each), variant 1 16 CTAs of 256 threads (16 rows each; a non-portable cluster size).
 using PlaneFY = LinePolicy<256>::F<true>;
 using PlaneFZ = LinePolicy<256>::F<false>;
-constexpr int kPlaneCL = 8;
-constexpr size_t plane_smem() {
-  constexpr int RZ = 256 / kPlaneCL, LY = KWB_PLANE_THREADS / PlaneFY::G, LZ = KWB_PLANE_THREADS / PlaneFZ::G;
+template <int CL, int THREADS>
+constexpr size_t plane_smem_of() {
+  constexpr int RZ = 256 / CL, LY = THREADS / PlaneFY::G, LZ = THREADS / PlaneFZ::G;
   constexpr int XS = (LY * PlaneFY::LP > LZ * PlaneFZ::LP) ? LY * PlaneFY::LP : LZ * PlaneFZ::LP;
   return ((size_t)RZ * 256 + XS + PlaneFY::TW + PlaneFZ::TW) * sizeof(float2);
 }
-static inline int plane_clusters_per_device() {
-  const void *fn = (const void *)k_plane_fast<PlaneFY, PlaneFZ, kPlaneCL>;
-  if (raise_smem(fn, plane_smem()) != cudaSuccess) return 0;
+template <int V> struct PlaneVariant;
+template <> struct PlaneVariant<0> {
+  static constexpr int CL = 8, THREADS = 512, MINB = 2;
+};
+template <> struct PlaneVariant<1> {
+  static constexpr int CL = 16, THREADS = 256, MINB = 4;
+};
+template <int V>
+inline const void *plane_fn() {
+  using P = PlaneVariant<V>;
+  return (const void *)k_plane_fast<PlaneFY, PlaneFZ, P::CL, P::THREADS, P::MINB>;
+}
+template <int V>
+inline cudaLaunchConfig_t plane_cfg(int n1, cudaStream_t st, cudaLaunchAttribute *at, bool pdl) {
+  using P = PlaneVariant<V>;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kPlaneCL * 16);
-  cfg.blockDim = dim3(KWB_PLANE_THREADS);
-  cfg.dynamicSmemBytes = plane_smem();
-  cudaLaunchAttribute at;
-  at.id = cudaLaunchAttributeClusterDimension;
-  at.val.clusterDim.x = kPlaneCL;
-  at.val.clusterDim.y = 1;
-  at.val.clusterDim.z = 1;
-  cfg.attrs = &at;
-  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(n1 * P::CL);
+  cfg.blockDim = dim3(P::THREADS);
+  cfg.dynamicSmemBytes = plane_smem_of<P::CL, P::THREADS>();
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = P::CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 2 : 1;
+  return cfg;
+}
+// Clusters of variant V that fit on the device at once (0: the variant is unavailable).
+template <int V>
+inline int plane_clusters_of() {
+  using P = PlaneVariant<V>;
+  const void *fn = plane_fn<V>();
+  if (raise_smem(fn, plane_smem_of<P::CL, P::THREADS>()) != cudaSuccess) return 0;
+  if (P::CL > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchAttribute at[2];
+  cudaLaunchConfig_t cfg = plane_cfg<V>(16, nullptr, at, false);
   int n = 0;
   if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return n;
+}
+static inline int plane_clusters_per_device() { return plane_clusters_of<0>(); }
+template <int V>
+inline cudaError_t plane_launch(const SimDev &h, long long s, cudaStream_t st) {
+  using P = PlaneVariant<V>;
+  cudaLaunchAttribute at[2];
+  cudaLaunchConfig_t cfg = plane_cfg<V>(h.n1, st, at, true);
+  return cudaLaunchKernelEx(&cfg, k_plane_fast<PlaneFY, PlaneFZ, P::CL, P::THREADS, P::MINB>, h, s);
 }
 
 // ------------------------------------------------------------------------------------------

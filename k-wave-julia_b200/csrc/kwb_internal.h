@@ -52,7 +52,7 @@ __host__ __device__ inline int fft_len(const FftPlan &p) { return p.m > 0 ? p.m 
 // Pass slots of the FFT schedule: line passes per axis, the x equation-of-state passes, the
 // y/z spectrum passes.
 enum { KWB_SLOT_LINE0 = 0, KWB_SLOT_LINE1 = 1, KWB_SLOT_LINE2 = 2, KWB_SLOT_EOS_FWD = 3, KWB_SLOT_EOS_INV = 4,
-       KWB_SLOT_SPEC1 = 5, KWB_SLOT_SPEC2 = 6, KWB_NSLOTS = 7 };
+       KWB_SLOT_SPEC1 = 5, KWB_SLOT_SPEC2 = 6, KWB_SLOT_PLANE = 7, KWB_NSLOTS = 8 };
 
 // Line-pass modes.
 enum { KWB_MODE_STEP = 0, KWB_MODE_INIT = 1 };
@@ -276,6 +276,7 @@ cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, lo
                       cudaStream_t st);
 bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
+int fast_plane_variants();
 void fast_plane_slot_ky(int Ny, int *ky);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
 

@@ -3,8 +3,8 @@
 // The reference plans its FFTs with FFTW's measured planning (plan_rfft(...; flags=FFTW.MEASURE),
 // KWave.jl/src/fft_utils.jl:59-60).  Here every pass of the time step has a few valid schedules
 // and the fastest is measured on first use of a grid shape:
-//   * register-FFT passes (power-of-two lines): the tile variant -- full-width tiles, 128-thread
-//     tiles or one-warp tiles;
+//   * register-FFT passes: the tile variant -- full-width tiles, 128-thread tiles or one-warp
+//     tiles -- and, for the 3-D cluster plane pass, 8 CTAs of 512 threads or 16 of 256 per plane;
 //   * Stockham passes (other lengths): the radix order of each axis's plan, the complex lines per
 //     tile, and the threads per CTA of the line passes.
 // Each candidate runs on the simulation's own buffers before its initial conditions are set
@@ -51,26 +51,25 @@ void schedule_apply(SimDev &h, const Schedule &s) {
 
 std::string schedule_str(const Schedule &s) {
   char buf[256];
-  snprintf(buf, sizeof(buf), "tile=%d,%d,%d,%d,%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d",
+  snprintf(buf, sizeof(buf), "tile=%d,%d,%d,%d,%d,%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d",
            s.tile_var[0], s.tile_var[1], s.tile_var[2], s.tile_var[3], s.tile_var[4], s.tile_var[5],
-           s.tile_var[6], s.thr_line[0], s.thr_line[1], s.thr_line[2], s.L_line[0], s.L_line[1],
+           s.tile_var[6], s.tile_var[7], s.thr_line[0], s.thr_line[1], s.thr_line[2], s.L_line[0], s.L_line[1],
            s.L_line[2], s.L_eosx, s.L_spec[1], s.L_spec[2], s.plan_order[0], s.plan_order[1],
            s.plan_order[2]);
   return buf;
 }
 
 bool schedule_parse(const char *txt, Schedule &s) {
-  int tv[7], th[3], L[6], po[3];
-  if (sscanf(txt, "tile=%d,%d,%d,%d,%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d", &tv[0],
-             &tv[1], &tv[2], &tv[3], &tv[4], &tv[5], &tv[6], &th[0], &th[1], &th[2], &L[0], &L[1], &L[2],
-             &L[3], &L[4], &L[5], &po[0], &po[1], &po[2]) != 19)
+  int tv[8], th[3], L[6], po[3];
+  if (sscanf(txt, "tile=%d,%d,%d,%d,%d,%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d", &tv[0],
+             &tv[1], &tv[2], &tv[3], &tv[4], &tv[5], &tv[6], &tv[7], &th[0], &th[1], &th[2], &L[0], &L[1],
+             &L[2], &L[3], &L[4], &L[5], &po[0], &po[1], &po[2]) != 20)
     return false;
   memset(&s, 0, sizeof(s));
-  for (int i = 0; i < 7; ++i) {
+  for (int i = 0; i < 8; ++i) {
     if (tv[i] < -1 || tv[i] > 2) return false;
     s.tile_var[i] = (signed char)tv[i];
   }
-  s.tile_var[7] = -1;
   for (int a = 0; a < 3; ++a) {
     if (th[a] < 0 || th[a] > KWB_PASS_THREADS_MAX || th[a] % 32) return false;
     if (po[a] < 0 || po[a] > 2) return false;
@@ -238,7 +237,13 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
     }
   }
 
-  // spectrum passes along y and z (the 3-D cluster plane pass has no variants)
+  // the 3-D cluster plane pass: 8 CTAs of 512 threads or 16 of 256 per kx plane
+  if (t.plane) {
+    const int nv = fast_plane_variants();
+    T.choose("plane", nv > 1 ? nv : 0, [&](int i) { t.tile_var[KWB_SLOT_PLANE] = (signed char)i; },
+             [&] { return fast_plane(d, t, 0, st); });
+  }
+  // spectrum passes along y and z
   if (!t.plane) {
     for (int a = 1; a < D; ++a) {
       auto go = [&, a] { return launch_spec_pass(d, t, a, KWB_SPEC_FWD_MUL_INV, 0, st); };

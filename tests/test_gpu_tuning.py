@@ -24,6 +24,7 @@ def _cases():
         "register_2d_256": c2(n=256, Nt=40, record=("p", "p_max", "p_rms")),
         "stockham_3d_48": c3(n=48, Nt=30, piston=8, pml=6),
         "stockham_3d_96": c3(n=96, Nt=20, piston=8, pml=6),
+        "plane_3d_256": c3(n=256, Nt=6),
     }
 
 
@@ -52,11 +53,12 @@ def _fields(out):
     return f
 
 
-@pytest.mark.parametrize("name", ["stockham_2d_270", "register_2d_256", "stockham_3d_48", "stockham_3d_96"])
+@pytest.mark.parametrize("name", ["stockham_2d_270", "register_2d_256", "stockham_3d_48", "stockham_3d_96",
+                                  "plane_3d_256"])
 def test_every_candidate_gives_the_same_fields(kb, name, monkeypatch):
-    """Candidates 0..3 of every pass (tile variants, lines per tile, threads per CTA): fields
-    bit-identical to the size heuristic's; the radix orders explored with KWB_TUNE_ORDER=1
-    agree to FP32 rounding."""
+    """Candidates 0..3 of every pass (tile variants, lines per tile, threads per CTA, the plane
+    pass's cluster shape): fields bit-identical to the size heuristic's; the radix orders
+    explored with KWB_TUNE_ORDER=1 agree to FP32 rounding."""
     case = _cases()[name]
     monkeypatch.setenv("KWB_TUNE", "0")
     ref, sched = _run(kb, case)
