@@ -1709,6 +1709,16 @@ struct LinePolicy<320> {
 };
 
 template <>
+struct LinePolicy<80> {
+  template <bool C> using F = LineFFT3G<20, 2, 2, C>;
+  static constexpr int THREADS = 128, MINB = 2;
+};
+template <>
+struct LinePolicy<640> {
+  template <bool C> using F = LineFFT4G<20, 4, 4, 2, C>;
+  static constexpr int THREADS = 256, MINB = 2;
+};
+template <>
 struct LinePolicy<384> {
   template <bool C> using F = LineFFT4G<12, 4, 4, 2, C>;
   static constexpr int THREADS = 256, MINB = 2;

@@ -1,13 +1,12 @@
-// Register-FFT kernels for the mixed-radix line lengths 96, 160, 192, 320 (LineFFT3G) and 384,
-// 768 (LineFFT4G), with a 12- or 20-point register DFT as the first level: the instantiations of
-// kwb_fast_impl.cuh's
+// Register-FFT kernels for the mixed-radix line lengths 96, 160, 192 and 320 (LineFFT3G, a 12-
+// or 20-point register DFT as the first level): the instantiations of kwb_fast_impl.cuh's
 // kernels for these lengths, in a translation unit of their own so that they compile alongside
 // the power-of-two ones.
 #include "kwb_fast_impl.cuh"
 
 namespace kwb {
 
-bool fast_mixed_size(int N) { return N == 96 || N == 160 || N == 192 || N == 320 || N == 384 || N == 768; }
+bool fast_mixed_size(int N) { return N == 96 || N == 160 || N == 192 || N == 320; }
 
 #define KWB_MIXED_SWITCH(N, FN, ARGS)      \
   switch (N) {                             \
@@ -15,8 +14,6 @@ bool fast_mixed_size(int N) { return N == 96 || N == 160 || N == 192 || N == 320
     case 160: return fast::FN<160> ARGS;   \
     case 192: return fast::FN<192> ARGS;   \
     case 320: return fast::FN<320> ARGS;   \
-    case 384: return fast::FN<384> ARGS;   \
-    case 768: return fast::FN<768> ARGS;   \
     default: return cudaErrorInvalidValue; \
   }
 

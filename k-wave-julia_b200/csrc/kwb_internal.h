@@ -257,7 +257,7 @@ cudaError_t launch_advance_t0(long long *t0, long long k, cudaStream_t st);
 cudaError_t prime_attributes(const SimDev &h);
 
 // Register-FFT kernels (kwb_fast.cu) for line lengths 64, 128, 256, 512, 1024, and (through
-// kwb_fast_mixed.cu) the mixed-radix lengths 96, 160, 192, 320.
+// kwb_fast_mixed.cu) the mixed-radix lengths 96, 160, 192, 320
 struct ElGrad;
 bool fast_size(int N);
 bool fast_mixed_size(int N);
@@ -268,6 +268,15 @@ cudaError_t fast_mixed_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long 
 cudaError_t fast_mixed_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
                             cudaStream_t st);
 cudaError_t fast_mixed_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
+// ... and (kwb_fast_mixed2.cu) 80, 384, 640, 768.
+bool fast_mixed2_size(int N);
+cudaError_t fast_mixed2_prime(int N);
+cudaError_t fast_mixed2_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                                  cudaStream_t st);
+cudaError_t fast_mixed2_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
+cudaError_t fast_mixed2_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                             cudaStream_t st);
+cudaError_t fast_mixed2_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
 cudaError_t fast_prime(int N);
 cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
                            cudaStream_t st);
