@@ -173,6 +173,13 @@ bool make_plan_order(int N, FftPlan &pl, int order) {
   if (order != 2)
     for (int i = 0; i < nodd; ++i)
       if (!push(odd[i])) return false;
+  // the stages' divisions by the butterflies per line and by the sub-transform length so far
+  int ns = 1;
+  for (int st = 0; st < pl.nstages; ++st) {
+    pl.div_nr[st] = make_fastdiv((unsigned)(N / pl.radix[st]));
+    pl.div_ns[st] = make_fastdiv((unsigned)ns);
+    ns *= pl.radix[st];
+  }
   return true;
 }
 

@@ -368,16 +368,7 @@ static int elementwise_grid(const SimDev &h) {
   return (int)std::max(1LL, std::min(want, cap));
 }
 
-static cudaError_t set_smem_optin(const void *fn, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
-  int dev = 0, optin = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (e != cudaSuccess) return e;
-  if (bytes > (size_t)optin) return cudaErrorInvalidValue;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-}
+static cudaError_t set_smem_optin(const void *fn, size_t bytes) { return raise_dynamic_smem(fn, bytes); }
 
 // Register-FFT passes serve power-of-two lines (strided ones need Nx a multiple of 4 for their
 // 16-byte staging); every other length runs on the Stockham kernel above.

@@ -1624,16 +1624,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 
 static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-static inline cudaError_t raise_smem(const void *fn, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
-  int dev = 0, optin = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (e != cudaSuccess) return e;
-  if (bytes > (size_t)optin) return cudaErrorInvalidValue;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-}
+static inline cudaError_t raise_smem(const void *fn, size_t bytes) { return raise_dynamic_smem(fn, bytes); }
 
 // Two compile-time tile sizes per line length: full tiles of 256/G complex lines for large
 // grids, and small tiles (one warp, >= 2 lines) when full tiles would leave SMs idle.

@@ -153,18 +153,24 @@ __host__ __device__ inline int line_pitch(int N) { return N + (N >> 4) + 1; }
 // use.
 __device__ __forceinline__ int spad(int m) { return m + (m >> 4); }
 
+__device__ __forceinline__ int fdiv(int n, FastDiv d) {
+  return (int)((__umulhi((unsigned)n, d.mul) + (unsigned)n) >> d.shift);
+}
+
 // One Stockham stage of radix R over L lines: X -> Y (pin / pout: X / Y in the padded layout).
+// dnr, dns: divisions by N / R and by Ns, precomputed in the plan.
 template <int R, bool INV>
 __device__ __forceinline__ void stockham_stage(const float2 *__restrict__ X, float2 *__restrict__ Y,
                                                int L, int LS, int N, int Ns,
-                                               const float2 *__restrict__ tw, bool pin, bool pout) {
+                                               const float2 *__restrict__ tw, bool pin, bool pout,
+                                               FastDiv dnr, FastDiv dns) {
   const int NR = N / R;
   const int total = L * NR;
   const int tstride = N / (Ns * R);
   for (int b = threadIdx.x; b < total; b += blockDim.x) {
-    const int l = b / NR;
+    const int l = fdiv(b, dnr);
     const int j = b - l * NR;
-    const int k = j % Ns;
+    const int k = j - fdiv(j, dns) * Ns;
     const float2 *x = X + l * LS;
     float2 *y = Y + l * LS;
     float2 v[R];
@@ -201,13 +207,14 @@ __device__ float2 *stockham_lines(float2 *X, float2 *Y, int L, int LS, const Fft
   for (int s = 0; s < plan.nstages; ++s) {
     const int R = plan.radix[s];
     const bool pin = s > 0, pout = s + 1 < plan.nstages;
+    const FastDiv dnr = plan.div_nr[s], dns = plan.div_ns[s];
     switch (R) {
-      case 2: stockham_stage<2, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
-      case 3: stockham_stage<3, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
-      case 4: stockham_stage<4, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
-      case 5: stockham_stage<5, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
-      case 7: stockham_stage<7, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
-      default: stockham_stage<8, INV>(X, Y, L, LS, N, Ns, tw, pin, pout); break;
+      case 2: stockham_stage<2, INV>(X, Y, L, LS, N, Ns, tw, pin, pout, dnr, dns); break;
+      case 3: stockham_stage<3, INV>(X, Y, L, LS, N, Ns, tw, pin, pout, dnr, dns); break;
+      case 4: stockham_stage<4, INV>(X, Y, L, LS, N, Ns, tw, pin, pout, dnr, dns); break;
+      case 5: stockham_stage<5, INV>(X, Y, L, LS, N, Ns, tw, pin, pout, dnr, dns); break;
+      case 7: stockham_stage<7, INV>(X, Y, L, LS, N, Ns, tw, pin, pout, dnr, dns); break;
+      default: stockham_stage<8, INV>(X, Y, L, LS, N, Ns, tw, pin, pout, dnr, dns); break;
     }
     __syncthreads();
     float2 *t = X;

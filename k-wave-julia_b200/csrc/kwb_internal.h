@@ -38,6 +38,17 @@
 // Bluestein's algorithm (chirp z-transform): m > 0 is the power-of-two length of the inner
 // transforms (m >= 2n - 1), the stages are m's, chirp[j] = exp(-i pi j^2 / n) (j < n) and
 // chirp_ft = FFT_m(conj chirp, wrapped) / m; m == 0 for a direct transform.
+// Division by a run-time constant d as a multiply and shift: n / d == (umulhi(n, mul) + n) >> shift
+// for 0 <= n < 2^31 (mul = floor(2^32 (2^shift - d) / d) + 1, shift = ceil(log2 d)).
+struct FastDiv {
+  unsigned mul;
+  unsigned shift;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  unsigned s = 0;
+  while ((1ull << s) < d) ++s;
+  return FastDiv{(unsigned)(((1ull << 32) * ((1ull << s) - d)) / d + 1), s};
+}
 struct FftPlan {
   int n;
   int nstages;
@@ -45,6 +56,10 @@ struct FftPlan {
   int m;
   const float2 *chirp;
   const float2 *chirp_ft;
+  // per stage: division by the butterflies per line (len / radix) and by the sub-transform
+  // length so far (the product of the earlier radices)
+  FastDiv div_nr[KWB_MAX_STAGES];
+  FastDiv div_ns[KWB_MAX_STAGES];
 };
 // Length of the transforms a plan runs (the buffers and twiddle table of a line are this long).
 __host__ __device__ inline int fft_len(const FftPlan &p) { return p.m > 0 ? p.m : p.n; }
@@ -225,6 +240,9 @@ struct GroupDev {
 
 // Kernel launchers (kwb_kernels.cu).
 namespace kwb {
+// Let kernel fn take `bytes` of dynamic shared memory: raises its limit to the device's opt-in
+// maximum less the kernel's own static shared memory (cudaErrorInvalidValue if bytes exceed it).
+cudaError_t raise_dynamic_smem(const void *fn, size_t bytes);
 // Stockham plan of a line of N points (false: a prime factor above 7 or too many stages), and
 // the complex lines per tile of a line pass (spec = false) or spectrum pass (spec = true) that
 // fit the shared-memory budget, at most cap_lines (kwb_api.cu).

@@ -542,16 +542,21 @@ int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile, int
 // The dynamic shared-memory limit of a kernel is a per-function attribute.  It is raised once to
 // the device's opt-in maximum, so simulations of different sizes in one process never lower
 // it under one another.
-static cudaError_t set_smem(const void *fn, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
+cudaError_t raise_dynamic_smem(const void *fn, size_t bytes) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  if (bytes + fa.sharedSizeBytes <= 48 * 1024) return cudaSuccess;
   int dev = 0, optin = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
-  if (bytes > (size_t)optin) return cudaErrorInvalidValue;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  const size_t room = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  if (bytes > room) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)room);
 }
+static cudaError_t set_smem(const void *fn, size_t bytes) { return raise_dynamic_smem(fn, bytes); }
 
 cudaError_t launch_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode,
                              long long step_s, cudaStream_t st) {

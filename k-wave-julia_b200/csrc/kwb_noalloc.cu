@@ -112,7 +112,8 @@ extern "C" int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t 
   for (int a = 0; a < 3; ++a) {
     const int64_t n = a < ndim ? N_in[a] : 1;
     if (n < 1 || n > KWB_MAX_N) return fail(KWB_E_UNSUPPORTED, "grid side outside 1..4096");
-    if (!make_plan((int)n, h.plan[a])) return fail(KWB_E_UNSUPPORTED, "grid side has a prime factor above 7");
+    if (!make_plan((int)n, h.plan[a]))
+      return fail(KWB_E_UNSUPPORTED, "grid side has a prime factor above 7 (no Bluestein transform without allocation)");
     h.N[a] = (int)n;
     if (a < ndim && !rho[a]) return fail(KWB_E_INVALID, "rho component pointer is NULL");
   }
