@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // thread's chunks differ by constants.
   auto stage = [&](float *dst, const float *f, int slot) {
     const float *fb = f + base;
-    if (CONTIG) {
+    if (CONTIG && S.tile_tma) {
       // rows contiguous in memory: one bulk copy of cnt rows (16-byte aligned: N % 4 == 0)
       if (tid == 0) {
         const unsigned bytes = (unsigned)cnt * N * 4u;
@@ -887,6 +887,14 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
         if (!(S.test_drop_copy && slot == 0 && blockIdx.x == 0)) bulk_copy_g2s(dst, fb, bytes, &tile_bar[slot]);
       }
       return;
+    } else if (CONTIG) {
+      constexpr int CH = 2 * L * N / 4, PER = (CH + THREADS - 1) / THREADS;  // rows contiguous in memory
+      const int chunks = cnt * N / 4;
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int q = tid + k * THREADS;
+        if (q < chunks) cp_async16(dst + 4 * q, fb + 4 * q, 16);
+      }
     } else {
       constexpr int CPR = (2 * L) / 4;  // 16-byte chunks per tile row (strided tiles have L >= 2)
       static_assert(THREADS % CPR == 0 && (CPR * N) % THREADS == 0, "strided staging");
@@ -907,6 +915,12 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // any copy still in flight before the CTA exits.
   bool issued[4] = {false, false, false, false};
   auto tile_wait = [&](int s0, int s1) -> bool {
+    if (!S.tile_tma) {  // 16-byte cp.async staging: the p tile alone first, then everything
+      if (s0 == 0 && s1 < 0) cp_async_wait<1>();
+      else cp_async_wait<0>();
+      __syncthreads();
+      return true;
+    }
     bool ok = true;
     if (s0 >= 0) ok = mbar_wait_bounded(&tile_bar[s0], 0) && ok;
     if (s1 >= 0) ok = mbar_wait_bounded(&tile_bar[s1], 0) && ok;
@@ -928,7 +942,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   if (rho0) {
     stage(st_r, rho0, 1);
     issued[1] = true;
-  } else if (!CONTIG) {
+  } else if (!CONTIG || !S.tile_tma) {
     cp_async_commit();
   }
   float2 *xs = sm + l * LP;

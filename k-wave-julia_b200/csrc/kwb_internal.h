@@ -170,6 +170,7 @@ struct SimDev {
   // complete); the host reads it after synchronising and reports KWB_E_DEVICE.
   int *err;
   int test_drop_copy;  // test hook: the first CTA of a contiguous line pass drops its p-tile copy
+  int tile_tma;        // contiguous line-pass tiles by bulk TMA copies (1) or 16-byte cp.async (0)
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
   // Measured FFT schedule (kwb_tune.cu): register-FFT tile variant per pass slot (KWB_SLOT_*;

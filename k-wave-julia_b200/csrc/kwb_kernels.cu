@@ -17,6 +17,8 @@
 // d, because the multiplier is Hermitian (it is real at the Nyquist bin).  Two real lines are
 // transformed as one complex line (a + i b) for the same reason.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "kwb_fft.cuh"
 #include "kwb_tiles.cuh"
@@ -543,18 +545,31 @@ int pass_threads(const SimDev &h, long long tiles, long long elems_per_tile, int
 // the device's opt-in maximum, so simulations of different sizes in one process never lower
 // it under one another.
 cudaError_t raise_dynamic_smem(const void *fn, size_t bytes) {
+  // the limit a kernel was given, per device: later calls that fit it make no API call
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> given;
+  int cur = 0;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(cur, fn);
+  auto it = given.find(key);
+  if (it != given.end() && bytes <= it->second) return cudaSuccess;
   cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  e = cudaFuncGetAttributes(&fa, fn);
   if (e != cudaSuccess) return e;
-  if (bytes + fa.sharedSizeBytes <= 48 * 1024) return cudaSuccess;
-  int dev = 0, optin = 0;
-  e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (bytes + fa.sharedSizeBytes <= 48 * 1024) {
+    given[key] = 48 * 1024 - fa.sharedSizeBytes;
+    return cudaSuccess;
+  }
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, cur);
   if (e != cudaSuccess) return e;
   const size_t room = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
   if (bytes > room) return cudaErrorInvalidValue;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)room);
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)room);
+  if (e == cudaSuccess) given[key] = room;
+  return e;
 }
 static cudaError_t set_smem(const void *fn, size_t bytes) { return raise_dynamic_smem(fn, bytes); }
 

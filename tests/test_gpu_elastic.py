@@ -152,7 +152,7 @@ def test_homogeneous_absorbing_2d_with_sources(kb, shape):
     assert_parity(out, ref, TOL_L2, TOL_MAX)
 
 
-@pytest.mark.parametrize("shape", [(128, 72), (64, 128)])
+@pytest.mark.parametrize("shape", [(128, 72), (64, 128), (160, 80), (80, 192)])
 def test_heterogeneous_2d(kb, shape):
     """Array speeds and density (no absorption in that branch), Dirichlet stress source, additive
     velocity source, p0."""
