@@ -6,8 +6,12 @@ B/A = 9 ball, 32x32 ux piston, xy-plane p + volume p_max), Nt = 1500, seeded syn
 A "step" is one time step of that simulation.  ``value`` is voxel-steps/s over K device-timed
 steps with all fields resident in HBM (CUDA events on the simulation's stream, max over ranks);
 ``e2e`` is one full solve through the public API from host arrays to FP64 outputs (wall clock,
-host<->device copies inside).  Multi-GPU: every rank runs its own independent simulation
-(weak scaling; simulations shard with no collective).
+host<->device copies inside), and ``accuracy`` compares that solve with the FP64 oracle's run of
+all 1500 steps (tests/golden/c3_long.npz).  Further keys: ``c2`` (the 512^2 x 2000-step solve,
+device-timed, with its accuracy against the oracle's 2000 steps), ``batch`` (64 mixed-size 2D
+simulations), ``serving`` (Poisson arrivals, p50/p99, sampled accuracy), ``elastic``,
+``comparators`` (the reference's step on cuFFT), ``cpu_baseline``.  Multi-GPU: every rank runs
+its own independent simulation (weak scaling; simulations shard with no collective).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c3|c2]
 """
@@ -27,11 +31,14 @@ sys.path.insert(0, os.path.join(ROOT, "k-wave-julia_b200"))
 # Spectral-pass-model words per voxel-step (algorithmic bytes = 4 B x words), per config.
 
 # DRAM bytes read + written (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# dominant kernel, from one `ncu --set full --clock-control none` capture of time step 2 of
-# `bench.py --steps 4 --warmup 3 --no-e2e --no-cpu --no-batch --no-serve` on a B200.  Reads
-# equal the algorithmic bytes; writes land lower because part of each launch's output is still
-# in L2 when the launch ends.
-NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 710.25e6}
+# dominant kernel, averaged over the launches of one capture on a B200:
+#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum
+#       --clock-control none -k regex:'k_line_fast|k_plane_fast|k_eos_inv_fast' -s 60 -c 10
+#       python bench.py --steps 4 --warmup 3 --no-e2e --no-cpu --no-batch --no-serve --no-elastic
+#       --no-cufft --no-c2
+# Reads equal the algorithmic bytes; writes land lower because part of each launch's output is
+# still in L2 when the launch ends.
+NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 706.2e6}
 
 SPM_WORDS = {"c3": 33.0, "c2": 26.0, "c1": 15.01}
 UNIT = "Gvoxel-steps/s"

@@ -375,6 +375,7 @@ def test_bounded_tile_wait_reports_an_error(kb, monkeypatch):
     word and returns, the host reports KWB_E_DEVICE, and the context keeps working."""
     from kwave_b200.workloads import c2
     monkeypatch.setenv("KWB_TUNE", "0")
+    monkeypatch.setenv("KWB_TILE_TMA", "1")
     monkeypatch.setenv("KWB_TEST_DROP_TILE_COPY", "1")
     case = c2(n=256, Nt=4, record=("p_max",))
     g, m, s, sen, kw = case.to_api()
