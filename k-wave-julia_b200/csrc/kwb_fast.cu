@@ -31,7 +31,8 @@ cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaSt
 }
 
 bool fast_size(int N) {
-  return N == 64 || N == 128 || N == 256 || N == 512 || N == 1024 || fast_mixed_size(N) || fast_mixed2_size(N);
+  return N == 64 || N == 128 || N == 256 || N == 512 || N == 1024 || fast_mixed_size(N) || fast_mixed2_size(N) ||
+         fast_mixed3_size(N) || fast_mixed4_size(N) || fast_mixed5_size(N);
 }
 
 #define KWB_LINE_SWITCH(N, FN, ARGS)       \
@@ -49,6 +50,9 @@ static cudaError_t prime_line(int N) { KWB_LINE_SWITCH(N, prime_line, ()) }
 cudaError_t fast_prime(int N) {
   if (fast_mixed_size(N)) return fast_mixed_prime(N);
   if (fast_mixed2_size(N)) return fast_mixed2_prime(N);
+  if (fast_mixed3_size(N)) return fast_mixed3_prime(N);
+  if (fast_mixed4_size(N)) return fast_mixed4_prime(N);
+  if (fast_mixed5_size(N)) return fast_mixed5_prime(N);
   cudaError_t e = prime_eos(N);
   return e != cudaSuccess ? e : prime_line(N);
 }
@@ -56,21 +60,33 @@ cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int m
                            cudaStream_t st) {
   if (fast_mixed_size(h.N[axis])) return fast_mixed_line_pass(d_sim, h, axis, mode, s, st);
   if (fast_mixed2_size(h.N[axis])) return fast_mixed2_line_pass(d_sim, h, axis, mode, s, st);
+  if (fast_mixed3_size(h.N[axis])) return fast_mixed3_line_pass(d_sim, h, axis, mode, s, st);
+  if (fast_mixed4_size(h.N[axis])) return fast_mixed4_line_pass(d_sim, h, axis, mode, s, st);
+  if (fast_mixed5_size(h.N[axis])) return fast_mixed5_line_pass(d_sim, h, axis, mode, s, st);
   KWB_LINE_SWITCH(h.N[axis], launch_line_n, (d_sim, h, axis, mode, s, st))
 }
 cudaError_t fast_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st) {
   if (fast_mixed_size(h.N[0])) return fast_mixed_eos(d_sim, h, fwd, s, st);
   if (fast_mixed2_size(h.N[0])) return fast_mixed2_eos(d_sim, h, fwd, s, st);
+  if (fast_mixed3_size(h.N[0])) return fast_mixed3_eos(d_sim, h, fwd, s, st);
+  if (fast_mixed4_size(h.N[0])) return fast_mixed4_eos(d_sim, h, fwd, s, st);
+  if (fast_mixed5_size(h.N[0])) return fast_mixed5_eos(d_sim, h, fwd, s, st);
   KWB_LINE_SWITCH(h.N[0], launch_eos_n, (d_sim, h, fwd, s, st))
 }
 cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s, cudaStream_t st) {
   if (fast_mixed_size(h.N[axis])) return fast_mixed_spec(d_sim, h, axis, op, s, st);
   if (fast_mixed2_size(h.N[axis])) return fast_mixed2_spec(d_sim, h, axis, op, s, st);
+  if (fast_mixed3_size(h.N[axis])) return fast_mixed3_spec(d_sim, h, axis, op, s, st);
+  if (fast_mixed4_size(h.N[axis])) return fast_mixed4_spec(d_sim, h, axis, op, s, st);
+  if (fast_mixed5_size(h.N[axis])) return fast_mixed5_spec(d_sim, h, axis, op, s, st);
   KWB_LINE_SWITCH(h.N[axis], launch_spec_n, (d_sim, h, axis, op, s, st))
 }
 cudaError_t fast_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st) {
   if (fast_mixed_size(h.N[axis])) return fast_mixed_el_grad(h, axis, g, s, st);
   if (fast_mixed2_size(h.N[axis])) return fast_mixed2_el_grad(h, axis, g, s, st);
+  if (fast_mixed3_size(h.N[axis])) return fast_mixed3_el_grad(h, axis, g, s, st);
+  if (fast_mixed4_size(h.N[axis])) return fast_mixed4_el_grad(h, axis, g, s, st);
+  if (fast_mixed5_size(h.N[axis])) return fast_mixed5_el_grad(h, axis, g, s, st);
   KWB_LINE_SWITCH(h.N[axis], launch_el_n, (h, axis, g, s, st))
 }
 

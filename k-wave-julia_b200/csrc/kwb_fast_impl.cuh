@@ -404,15 +404,16 @@ struct LineFFT3 {
 };
 
 // LineFFT3 for mixed-radix lengths: N = R1 * A * B with R1 = 12 or 20 (a register DFT of 3 or 5
-// times a power of two) and A, B powers of two dividing R1, e.g. 96 = 12*2*4, 192 = 12*4*4,
-// 160 = 20*2*4, 320 = 20*4*4.  Same three levels and the same register layouts as LineFFT3;
-// the exchange buffers use generic padding (odd pitches) instead of LineFFT3's tuned offsets, and
-// the natural-order slots pad one per 32.
+// times a power of two) and A, B dividing R1 (register DFTs of 2, 3, 4, 5, 6, 10 or 12 points),
+// e.g. 96 = 12*2*4, 192 = 12*4*4, 160 = 20*2*4, 320 = 20*4*4, 288 = 12*4*6, 1000 = 20*5*10.
+// Same three levels and the same register layouts as LineFFT3; the exchange buffers use generic
+// padding (odd pitches) instead of LineFFT3's tuned offsets, and the natural-order slots pad one
+// per 32.  With G = A*B not dividing 32, a line's threads span warps and WARP must be false.
 template <int R1, int A, int B, bool WARP>
 struct LineFFT3G {
   static constexpr int E = R1, G = A * B, N = R1 * A * B;
   static constexpr int P2 = R1 / B, P3 = R1 / A;
-  static_assert(R1 % A == 0 && R1 % B == 0 && (A & (A - 1)) == 0 && (B & (B - 1)) == 0, "LineFFT3G shape");
+  static_assert(R1 % A == 0 && R1 % B == 0, "LineFFT3G shape: A and B divide R1");
   static constexpr int RP = G + 1;   // level-1 twiddle pitch
   static constexpr int AP = A + 1;   // level-2 twiddle pitch
   static constexpr int RP1 = G + 1;  // level-1 exchange [q][u]
@@ -456,7 +457,7 @@ struct LineFFT3G {
       float2 w[B];
 #pragma unroll
       for (int b = 0; b < B; ++b) w[b] = xs[i1(q1, a + A * b)];
-      dft_reg<B, false>(w);
+      dft_mixed<B, false>(w);
 #pragma unroll
       for (int mb = 0; mb < B; ++mb) v[j * B + mb] = mb == 0 ? w[mb] : cmul(w[mb], tw[R1 * RP + mb * AP + a]);
     }
@@ -474,7 +475,7 @@ struct LineFFT3G {
       float2 w[A];
 #pragma unroll
       for (int a = 0; a < A; ++a) w[a] = xs[i2(q1, mb, a)];
-      dft_reg<A, false>(w);
+      dft_mixed<A, false>(w);
 #pragma unroll
       for (int ma = 0; ma < A; ++ma) v[j * A + ma] = w[ma];
     }
@@ -488,7 +489,7 @@ struct LineFFT3G {
       float2 w[A];
 #pragma unroll
       for (int ma = 0; ma < A; ++ma) w[ma] = v[j * A + ma];
-      dft_reg<A, true>(w);
+      dft_mixed<A, true>(w);
 #pragma unroll
       for (int a = 0; a < A; ++a) xs[i2(q1, mb, a)] = w[a];
     }
@@ -499,7 +500,7 @@ struct LineFFT3G {
       float2 w[B];
 #pragma unroll
       for (int mb = 0; mb < B; ++mb) w[mb] = mb == 0 ? xs[i2(q1, mb, a)] : cmul_conj(xs[i2(q1, mb, a)], tw[R1 * RP + mb * AP + a]);
-      dft_reg<B, true>(w);
+      dft_mixed<B, true>(w);
 #pragma unroll
       for (int b = 0; b < B; ++b) v[j * B + b] = w[b];
     }
@@ -1723,6 +1724,53 @@ struct LinePolicy<640> {
   template <bool C> using F = LineFFT4G<20, 4, 4, 2, C>;
   static constexpr int THREADS = 256, MINB = 2;
 };
+// Threads per line not a power of two (block-level exchanges); THREADS keeps the full-width tile
+// at an even number of lines.
+template <>
+struct LinePolicy<144> {
+  template <bool C> using F = LineFFT3G<12, 3, 4, false>;
+  static constexpr int THREADS = 192, MINB = 2;
+};
+template <>
+struct LinePolicy<288> {
+  template <bool C> using F = LineFFT3G<12, 4, 6, false>;
+  static constexpr int THREADS = 192, MINB = 2;
+};
+template <>
+struct LinePolicy<432> {
+  template <bool C> using F = LineFFT3G<12, 6, 6, false>;
+  static constexpr int THREADS = 288, MINB = 2;
+};
+template <>
+struct LinePolicy<576> {
+  template <bool C> using F = LineFFT3G<12, 4, 12, false>;
+  static constexpr int THREADS = 192, MINB = 2;
+};
+template <>
+struct LinePolicy<864> {
+  template <bool C> using F = LineFFT3G<12, 6, 12, false>;
+  static constexpr int THREADS = 288, MINB = 2;
+};
+template <>
+struct LinePolicy<400> {
+  template <bool C> using F = LineFFT3G<20, 4, 5, false>;
+  static constexpr int THREADS = 160, MINB = 2;
+};
+template <>
+struct LinePolicy<500> {
+  template <bool C> using F = LineFFT3G<20, 5, 5, false>;
+  static constexpr int THREADS = 200, MINB = 2;
+};
+template <>
+struct LinePolicy<800> {
+  template <bool C> using F = LineFFT3G<20, 4, 10, false>;
+  static constexpr int THREADS = 160, MINB = 2;
+};
+template <>
+struct LinePolicy<1000> {
+  template <bool C> using F = LineFFT3G<20, 5, 10, false>;
+  static constexpr int THREADS = 200, MINB = 2;
+};
 template <>
 struct LinePolicy<384> {
   template <bool C> using F = LineFFT4G<12, 4, 4, 2, C>;
@@ -1761,7 +1809,7 @@ static inline cudaError_t prime_line() {
   if ((e = prime_line_variant<N, false, BIG>()) != cudaSuccess) return e;
   if ((e = prime_line_variant<N, true, SMALL>()) != cudaSuccess) return e;
   if ((e = prime_line_variant<N, false, SMALL>()) != cudaSuccess) return e;
-  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  constexpr int MID = ((128 / G) & ~1) > SMALL ? ((128 / G) & ~1) : SMALL;  // even line counts
   if ((e = prime_line_variant<N, true, MID>()) != cudaSuccess) return e;
   return prime_line_variant<N, false, MID>();
 }
@@ -1788,7 +1836,7 @@ static inline cudaError_t launch_line_n(const SimDev *d_sim, const SimDev &h, in
   using P = LinePolicy<N>;
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
-  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  constexpr int MID = ((128 / G) & ~1) > SMALL ? ((128 / G) & ~1) : SMALL;  // even line counts
   const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * BIG) * h.N[2]
                                     : (long long)cdiv(h.N[0], 2 * BIG) * (axis == 1 ? h.N[2] : h.N[1]);
   switch (tile_variant(h, KWB_SLOT_LINE0 + axis, tiles)) {
@@ -1822,7 +1870,7 @@ static inline cudaError_t prime_eos_n() {
   using P = LinePolicy<N>;
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
-  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  constexpr int MID = ((128 / G) & ~1) > SMALL ? ((128 / G) & ~1) : SMALL;  // even line counts
   cudaError_t e = prime_eos_variant<N, BIG>();
   if (e == cudaSuccess) e = prime_eos_variant<N, MID>();
   return e != cudaSuccess ? e : prime_eos_variant<N, SMALL>();
@@ -1847,7 +1895,7 @@ static inline cudaError_t launch_eos_n(const SimDev *d_sim, const SimDev &h, boo
   using P = LinePolicy<N>;
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
-  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  constexpr int MID = ((128 / G) & ~1) > SMALL ? ((128 / G) & ~1) : SMALL;  // even line counts
   switch (tile_variant(h, fwd ? KWB_SLOT_EOS_FWD : KWB_SLOT_EOS_INV, (long long)cdiv(h.N[1], 2 * BIG) * h.N[2])) {
     case 1: eos_go<N, MID>(d_sim, h, fwd, s, st); break;
     case 2: eos_go<N, SMALL>(d_sim, h, fwd, s, st); break;
@@ -1870,7 +1918,7 @@ static inline cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, in
   using P = LinePolicy<N>;
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
-  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  constexpr int MID = ((128 / G) & ~1) > SMALL ? ((128 / G) & ~1) : SMALL;  // even line counts
   switch (tile_variant(h, KWB_SLOT_SPEC1 + axis - 1, (long long)cdiv(h.n1, BIG) * (axis == 1 ? h.N[2] : h.N[1]))) {
     case 1: spec_go<N, MID>(d_sim, h, axis, op, s, st); break;
     case 2: spec_go<N, SMALL>(d_sim, h, axis, op, s, st); break;
@@ -2098,7 +2146,7 @@ static inline cudaError_t launch_el_n(const SimDev &h, int axis, const ElGrad &g
   using P = LinePolicy<N>;
   constexpr int G = P::template F<true>::G;
   constexpr int BIG = P::THREADS / G, SMALL = (32 / G > 2 ? 32 / G : 2);
-  constexpr int MID = (128 / G > SMALL ? 128 / G : SMALL);
+  constexpr int MID = ((128 / G) & ~1) > SMALL ? ((128 / G) & ~1) : SMALL;  // even line counts
   const long long tiles = axis == 0 ? (long long)cdiv(h.N[1], 2 * BIG) * h.N[2]
                                     : (long long)cdiv(h.N[0], 2 * BIG) * (axis == 1 ? h.N[2] : h.N[1]);
   switch (tile_variant(h, KWB_SLOT_LINE0 + axis, tiles)) {

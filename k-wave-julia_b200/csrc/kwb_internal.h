@@ -296,6 +296,33 @@ cudaError_t fast_mixed2_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long
 cudaError_t fast_mixed2_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
                              cudaStream_t st);
 cudaError_t fast_mixed2_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
+// ... (kwb_fast_mixed3.cu) 144, 288, 432.
+bool fast_mixed3_size(int N);
+cudaError_t fast_mixed3_prime(int N);
+cudaError_t fast_mixed3_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                                  cudaStream_t st);
+cudaError_t fast_mixed3_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
+cudaError_t fast_mixed3_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                             cudaStream_t st);
+cudaError_t fast_mixed3_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
+// ... (kwb_fast_mixed4.cu) 576, 864, 400.
+bool fast_mixed4_size(int N);
+cudaError_t fast_mixed4_prime(int N);
+cudaError_t fast_mixed4_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                                  cudaStream_t st);
+cudaError_t fast_mixed4_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
+cudaError_t fast_mixed4_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                             cudaStream_t st);
+cudaError_t fast_mixed4_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
+// ... (kwb_fast_mixed5.cu) 500, 800, 1000.
+bool fast_mixed5_size(int N);
+cudaError_t fast_mixed5_prime(int N);
+cudaError_t fast_mixed5_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
+                                  cudaStream_t st);
+cudaError_t fast_mixed5_eos(const SimDev *d_sim, const SimDev &h, bool fwd, long long s, cudaStream_t st);
+cudaError_t fast_mixed5_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, long long s,
+                             cudaStream_t st);
+cudaError_t fast_mixed5_el_grad(const SimDev &h, int axis, const ElGrad &g, long long s, cudaStream_t st);
 cudaError_t fast_prime(int N);
 cudaError_t fast_line_pass(const SimDev *d_sim, const SimDev &h, int axis, int mode, long long s,
                            cudaStream_t st);

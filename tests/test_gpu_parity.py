@@ -436,9 +436,11 @@ def _p0_case(shape, seed, Nt, pml=8, record=("p_final", "p_max", "p_rms")):
 @pytest.mark.parametrize("shape", [(1024, 64), (64, 1024), (512, 128), (128, 512), (64, 64, 64), (32, 256, 32),
                                    (64, 256, 256), (192, 96), (96, 192), (160, 320), (320, 160), (96, 96, 96),
                                    (192, 64, 160), (64, 320, 192), (384, 64), (64, 384), (768, 96), (96, 768),
-                                   (384, 32, 64), (640, 80), (80, 640), (80, 80, 80)])
+                                   (384, 32, 64), (640, 80), (80, 640), (80, 80, 80), (288, 400), (400, 288),
+                                   (432, 500), (500, 432), (576, 64), (64, 576), (864, 96), (96, 864), (800, 64),
+                                   (64, 800), (1000, 64), (64, 1000), (144, 144, 48), (48, 144, 64)])
 def test_register_fft_sizes(kb, shape):
-    """Every register-FFT line length (64..1024 and the mixed-radix 80, 96, 160, 192, 320, 384, 640, 768) on the
+    """Every register-FFT line length (64..1024 and the mixed-radix 80, 96, 144, 160, 192, 288, 320, 384, 400, 432, 500, 576, 640, 768, 800, 864, 1000) on the
     contiguous x axis and strided axes; (64, 256, 256) takes the cluster plane pass for the y/z
     spectrum transforms."""
     case = _p0_case(shape, sum(shape), Nt=60)
