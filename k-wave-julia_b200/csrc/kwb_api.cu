@@ -1063,6 +1063,8 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     h.test_drop_copy = dc && strcmp(dc, "1") == 0;
     const char *tt = getenv("KWB_TILE_TMA");  // 0: contiguous tiles by 16-byte cp.async instead
     h.tile_tma = !(tt && strcmp(tt, "0") == 0);
+    const char *ep = getenv("KWB_EOS_PREFETCH");  // 0: no L2 prefetch of the EOS operands
+    h.eos_prefetch = !(ep && strcmp(ep, "0") == 0);
   }
   CU(M.alloc(&h.p, nvox));
   CU(cudaMemsetAsync(h.p, 0, nvox * 4, st));

@@ -765,6 +765,10 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsign
                "l"(src), "r"(bytes), "r"(smem_u32(m))
                : "memory");
 }
+// Bulk prefetch of a contiguous block into L2 (16-byte aligned address and size).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *m, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -1021,6 +1025,19 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   __syncthreads();  // every thread is done with the velocity tile
   stage(st_p, S.rho[axis], 3);
   issued[3] = true;
+  if constexpr (XEOS) {
+    // the equation-of-state operands of this tile (rho_y, rho_z, the B/A term, c^2) are read
+    // after the density update; each is one contiguous block, prefetched into L2 now so that
+    // those loads hit L2 instead of waiting on HBM
+    if (S.eos_prefetch && tid == 0) {
+      const unsigned bytes = (unsigned)cnt * N * 4u;
+      const float *ops[4] = {S.D > 1 ? S.rho[1] : nullptr, S.D > 2 ? S.rho[2] : nullptr,
+                             S.nonlinear ? S.nlq : nullptr, S.c0sq};
+#pragma unroll
+      for (int f = 0; f < 4; ++f)
+        if (ops[f]) bulk_prefetch_l2(ops[f] + base, bytes);
+    }
+  }
 
   // velocity sources on this tile's lines (first_order_steps.jl:586-617, 646-690)
   // (entries are sorted by line: a thread scans only its own two lines)

@@ -171,6 +171,7 @@ struct SimDev {
   int *err;
   int test_drop_copy;  // test hook: the first CTA of a contiguous line pass drops its p-tile copy
   int tile_tma;        // contiguous line-pass tiles by bulk TMA copies (1) or 16-byte cp.async (0)
+  int eos_prefetch;    // the fused x pass prefetches its equation-of-state operands into L2
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
   // Measured FFT schedule (kwb_tune.cu): register-FFT tile variant per pass slot (KWB_SLOT_*;
