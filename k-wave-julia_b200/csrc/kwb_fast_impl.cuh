@@ -1567,6 +1567,10 @@ __global__ void __launch_bounds__(THREADS, MINB)
   const unsigned rank = cluster_rank();
   const int kx = blockIdx.x / CL;
   const int tid = threadIdx.x;
+  // the multiplier of plane kx is read in the z phase; each CTA prefetches its slice of it (rows
+  // k_z in [rank RZ, (rank+1) RZ), contiguous) into L2 now, so that the cluster holds all of it
+  if (S.eos_prefetch && tid == 0)
+    bulk_prefetch_l2(S.M + ((long long)kx * NZ + (long long)rank * RZ) * NY, (unsigned)(RZ * NY * 4));
   const long long rstride = (long long)S.n1 * NY;  // between consecutive z rows of the plane
   float2 *plane = S.spec + (long long)rank * RZ * rstride + (long long)kx * NY;
   // rows in two groups, so that the first transforms start while the second group lands
