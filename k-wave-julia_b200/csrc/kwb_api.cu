@@ -1523,6 +1523,14 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if ((rc = choose_schedule(S.get(), h, st))) return rc;
     CU(prime_attributes(h));
   }
+  if (h.plane && fast_plane_slot_major(h)) {
+    // the slot-major plane pass reads its multiplier as [kx][slot][k_z in register order]
+    TempBuf tmp(st, ctx->pool);
+    float *Mk;
+    CU(tmp.alloc(&Mk, h.nspec));
+    CU(cudaMemcpyAsync(Mk, h.M, h.nspec * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CU(fast_plane_relayout(const_cast<float *>(h.M), Mk, h.n1, st));
+  }
 
   // ---- device descriptor
   CU(M.alloc(&S->d_sim, 1));

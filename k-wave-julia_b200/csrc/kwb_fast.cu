@@ -12,22 +12,77 @@ bool fast_plane_available() {
   if (n < 0) n = fast::plane_clusters_per_device();
   return n > 0;
 }
-// Plane-pass variants usable on this device (1 or 2: the 16-CTA clusters need the non-portable
-// cluster size).
-int fast_plane_variants() {
-  static int v = -1;
-  if (v < 0) v = !fast_plane_available() ? 0 : (fast::plane_clusters_of<1>() > 0 ? 2 : 1);
-  return v;
+// Plane-pass variants usable on this device, in the order the tuner tries them (their ids in
+// ids[]; 16-CTA clusters need the non-portable cluster size).
+int fast_plane_variants(int *ids) {
+  static int n = -1, v[4];
+  if (n < 0) {
+    int k = 0;
+    if (fast_plane_available()) {
+      v[k++] = 0;
+      if (fast::plane_clusters_of<2>() > 0) v[k++] = 2;
+      if (fast::plane_clusters_of<1>() > 0) v[k++] = 1;
+      if (fast::plane_clusters_of<3>() > 0) v[k++] = 3;
+    }
+    n = k;
+  }
+  if (ids)
+    for (int i = 0; i < n; ++i) ids[i] = v[i];
+  return n;
 }
+// The variant a simulation runs: its measured choice, else slot-major 8 x 512 (108 vs 112 µs per
+// 256^3 launch for row-major 8 x 512, 117 and 127 µs for the 16-CTA shapes), else row-major.
+static int plane_variant_of(const SimDev &h) {
+  int ids[4];
+  const int n = fast_plane_variants(ids);
+  const int want = h.tile_var[KWB_SLOT_PLANE] >= 0 ? h.tile_var[KWB_SLOT_PLANE] : 2;
+  for (int i = 0; i < n; ++i)
+    if (ids[i] == want) return want;
+  return 0;
+}
+// Shared-memory and cluster-size attributes of the usable variants on the current device (a
+// function attribute is set per device).
+template <int V>
+static cudaError_t plane_prime_one() {
+  using P = fast::PlaneVariant<V>;
+  const void *fn = fast::plane_fn<V>();
+  cudaError_t e = raise_dynamic_smem(fn, fast::plane_smem_of<V>());
+  if (e == cudaSuccess && P::CL > 8) e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+cudaError_t fast_plane_prime() {
+  int ids[4];
+  const int n = fast_plane_variants(ids);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    switch (ids[i]) {
+      case 1: e = plane_prime_one<1>(); break;
+      case 2: e = plane_prime_one<2>(); break;
+      case 3: e = plane_prime_one<3>(); break;
+      default: e = plane_prime_one<0>(); break;
+    }
+  }
+  return e;
+}
+bool fast_plane_slot_major(const SimDev &h) { return h.plane && plane_variant_of(h) >= 2; }
 // Register-order slot -> k_y of the plane pass's y transform (the layout of its multiplier).
 void fast_plane_slot_ky(int Ny, int *ky) {
   using F = fast::PlaneFY;
   for (int s = 0; s < Ny; ++s) ky[s] = F::k_of(s % F::G, s / F::G);
 }
+cudaError_t fast_plane_relayout(float *M, const float *M_kz_slot, int n1, cudaStream_t st) {
+  const long long total = (long long)n1 * 256 * 256;
+  fast::k_plane_m_cols<fast::PlaneFY><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(M, M_kz_slot, total);
+  return cudaGetLastError();
+}
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
   (void)d_sim;
-  const int v = h.tile_var[KWB_SLOT_PLANE] == 1 && fast_plane_variants() > 1 ? 1 : 0;
-  return v == 1 ? fast::plane_launch<1>(h, s, st) : fast::plane_launch<0>(h, s, st);
+  switch (plane_variant_of(h)) {
+    case 1: return fast::plane_launch<1>(h, s, st);
+    case 2: return fast::plane_launch<2>(h, s, st);
+    case 3: return fast::plane_launch<3>(h, s, st);
+    default: return fast::plane_launch<0>(h, s, st);
+  }
 }
 
 bool fast_size(int N) {

@@ -1654,6 +1654,110 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
 }
 
+// Plane pass with slot-major rows: the same three steps and the same arithmetic as k_plane_fast,
+// with one warp per line throughout and no block-wide barriers.  After its y transforms a CTA
+// stores its rows slot-major, cols[slot][z row] with an odd pitch RZ + 1, so the part of the z
+// line of one slot that a cluster CTA holds is RZ consecutive values: the warp that owns the line
+// gathers it with contiguous distributed-shared-memory reads (lane t takes z = t + 32 r from CTA
+// z / RZ, row z % RZ), transforms it, multiplies, transforms back and scatters it to the same
+// places.  Each slot column of a CTA is touched by exactly one warp of the cluster between the
+// two cluster barriers, so nothing else orders the z step.  Rows are read from and written to
+// the plane directly (lane t holds x[t + 32 r]: coalesced 256-byte row segments).  The multiplier
+// is laid out [kx][slot][j] with k_z = F::k_of(j % 32, j / 32), so a line's 256 values are
+// contiguous (fast_plane_relayout).
+template <class F, int CL, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_plane_cols(const __grid_constant__ SimDev S, long long step_s) {
+  constexpr int NY = F::N, NZ = F::N, RZ = NZ / CL, CY = NY / CL, W = THREADS / 32;
+  constexpr int RP = RZ + 1;  // pitch of a slot column (odd: conflict-free row stores)
+  static_assert(F::G == 32 && F::WARP_SYNC, "one warp per line");
+  static_assert(RZ % W == 0 && CY % W == 0 && NZ % RZ == 0, "plane tiling");
+  extern __shared__ float4 smem_raw[];
+  float2 *cols = reinterpret_cast<float2 *>(smem_raw);  // [NY][RP]
+  float2 *xsb = cols + NY * RP;                          // one exchange buffer per warp
+  float2 *twy = xsb + W * F::LP;
+  float2 *twz = twy + F::TW;
+  F::build_tw(twy, S.tw[1]);
+  F::build_tw(twz, S.tw[2]);
+  KWB_STEP_KERNEL_PROLOGUE();
+  const long long t = *S.t0 + step_s;
+  if (t >= S.Nt) return;  // uniform over the cluster
+  const unsigned rank = cluster_rank();
+  const int kx = blockIdx.x / CL;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float2 *xs = xsb + w * F::LP;
+  const float *__restrict__ Mk = S.M + (long long)kx * NY * NZ;
+  if (S.eos_prefetch && threadIdx.x == 0) bulk_prefetch_l2(Mk + (long long)rank * CY * NZ, (unsigned)(CY * NZ * 4));
+  const long long rstride = (long long)S.n1 * NY;  // between consecutive z rows of the plane
+  float2 *plane = S.spec + (long long)rank * RZ * rstride + (long long)kx * NY;
+  __syncthreads();  // twiddles
+
+  // 1. forward along y, rows to slot-major columns
+#pragma unroll 1
+  for (int zl = w; zl < RZ; zl += W) {
+    const float2 *row = plane + zl * rstride;
+    float2 v[F::E];
+#pragma unroll
+    for (int r = 0; r < F::E; ++r) v[r] = row[lane + 32 * r];
+    F::fwd(v, xs, twy, lane);
+#pragma unroll
+    for (int idx = 0; idx < F::E; ++idx) cols[(lane + 32 * idx) * RP + zl] = v[idx];
+  }
+  cluster_barrier();
+
+  // 2. the z lines of this CTA's slots: gather, forward, multiply, back, scatter
+  const unsigned cbase = cta_smem_addr(cols);
+#pragma unroll 1
+  for (int c = w; c < CY; c += W) {
+    const int sl = (int)rank * CY + c;
+    float2 v[F::E];
+#pragma unroll
+    for (int r = 0; r < F::E; ++r) {
+      const int z = lane + 32 * r;
+      v[r] = cluster_ld(cluster_map(cbase + (unsigned)((sl * RP + z % RZ) * 8), (unsigned)(z / RZ)));
+    }
+    F::fwd(v, xs, twz, lane);
+    const float *m = Mk + (long long)sl * NZ + lane;
+#pragma unroll
+    for (int idx = 0; idx < F::E; ++idx) {
+      const float mm = __ldg(m + 32 * idx);
+      v[idx] = make_float2(v[idx].x * mm, v[idx].y * mm);
+    }
+    F::inv(v, xs, twz, lane);
+#pragma unroll
+    for (int r = 0; r < F::E; ++r) {
+      const int z = lane + 32 * r;
+      cluster_st(cluster_map(cbase + (unsigned)((sl * RP + z % RZ) * 8), (unsigned)(z / RZ)), v[r]);
+    }
+  }
+  cluster_barrier();
+
+  // 3. back along y, straight to the plane
+#pragma unroll 1
+  for (int zl = w; zl < RZ; zl += W) {
+    float2 v[F::E];
+#pragma unroll
+    for (int idx = 0; idx < F::E; ++idx) v[idx] = cols[(lane + 32 * idx) * RP + zl];
+    F::inv(v, xs, twy, lane);
+    float2 *out = plane + zl * rstride;
+#pragma unroll
+    for (int r = 0; r < F::E; ++r) out[lane + 32 * r] = v[r];
+  }
+}
+
+// Multiplier of the slot-major plane pass, [kx][slot][j] with k_z = F::k_of(j % 32, j / 32), from
+// the [kx][k_z][slot] layout the table builder writes.
+template <class F>
+__global__ void k_plane_m_cols(float *__restrict__ out, const float *__restrict__ in, long long total) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  constexpr int N = F::N;
+  const int j = (int)(i % N), s = (int)((i / N) % N);
+  const long long kx = i / ((long long)N * N);
+  const int kz = F::k_of(j % 32, j / 32);
+  out[i] = in[(kx * N + kz) * N + s];
+}
+
 // ------------------------------------------------------------------------------------------
 // dispatch
 // ------------------------------------------------------------------------------------------
@@ -1948,27 +2052,52 @@ static inline cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, in
   return cudaGetLastError();
 }
 
-// Cluster plane pass for Ny = Nz = 256: variant 0 has 8 CTAs of 512 threads per kx plane (32 rows
-// each), variant 1 16 CTAs of 256 threads (16 rows each; a non-portable cluster size).
+// Cluster plane pass for Ny = Nz = 256.  Variants: 0 -- k_plane_fast with 8 CTAs of 512 threads
+// per kx plane (32 rows each); 1 -- k_plane_fast with 16 CTAs of 256 threads (16 rows each; a
+// non-portable cluster size); 2 and 3 -- k_plane_cols with the same two cluster shapes (its
+// multiplier in the slot-major layout).
 using PlaneFY = LinePolicy<256>::F<true>;
 using PlaneFZ = LinePolicy<256>::F<false>;
-template <int CL, int THREADS>
-constexpr size_t plane_smem_of() {
-  constexpr int RZ = 256 / CL, LY = THREADS / PlaneFY::G, LZ = THREADS / PlaneFZ::G;
-  constexpr int XS = (LY * PlaneFY::LP > LZ * PlaneFZ::LP) ? LY * PlaneFY::LP : LZ * PlaneFZ::LP;
-  return ((size_t)RZ * 256 + XS + PlaneFY::TW + PlaneFZ::TW) * sizeof(float2);
-}
 template <int V> struct PlaneVariant;
 template <> struct PlaneVariant<0> {
   static constexpr int CL = 8, THREADS = 512, MINB = 2;
+  static constexpr bool COLS = false;
 };
 template <> struct PlaneVariant<1> {
   static constexpr int CL = 16, THREADS = 256, MINB = 4;
+  static constexpr bool COLS = false;
+};
+template <> struct PlaneVariant<2> {
+  static constexpr int CL = 8, THREADS = 512, MINB = 2;
+  static constexpr bool COLS = true;
+};
+template <> struct PlaneVariant<3> {
+  static constexpr int CL = 16, THREADS = 256, MINB = 3;
+  static constexpr bool COLS = true;
 };
 template <int V>
-inline const void *plane_fn() {
+constexpr size_t plane_smem_of() {
   using P = PlaneVariant<V>;
-  return (const void *)k_plane_fast<PlaneFY, PlaneFZ, P::CL, P::THREADS, P::MINB>;
+  constexpr int RZ = 256 / P::CL;
+  if (P::COLS) {
+    constexpr int W = P::THREADS / 32;
+    return ((size_t)256 * (RZ + 1) + W * PlaneFY::LP + 2 * PlaneFY::TW) * sizeof(float2);
+  }
+  constexpr int LY = P::THREADS / PlaneFY::G, LZ = P::THREADS / PlaneFZ::G;
+  constexpr int XS = (LY * PlaneFY::LP > LZ * PlaneFZ::LP) ? LY * PlaneFY::LP : LZ * PlaneFZ::LP;
+  return ((size_t)RZ * 256 + XS + PlaneFY::TW + PlaneFZ::TW) * sizeof(float2);
+}
+template <int V>
+inline auto plane_kernel() {
+  using P = PlaneVariant<V>;
+  if constexpr (P::COLS)
+    return k_plane_cols<PlaneFY, P::CL, P::THREADS, P::MINB>;
+  else
+    return k_plane_fast<PlaneFY, PlaneFZ, P::CL, P::THREADS, P::MINB>;
+}
+template <int V>
+inline const void *plane_fn() {
+  return (const void *)plane_kernel<V>();
 }
 template <int V>
 inline cudaLaunchConfig_t plane_cfg(int n1, cudaStream_t st, cudaLaunchAttribute *at, bool pdl) {
@@ -1976,7 +2105,7 @@ inline cudaLaunchConfig_t plane_cfg(int n1, cudaStream_t st, cudaLaunchAttribute
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(n1 * P::CL);
   cfg.blockDim = dim3(P::THREADS);
-  cfg.dynamicSmemBytes = plane_smem_of<P::CL, P::THREADS>();
+  cfg.dynamicSmemBytes = plane_smem_of<V>();
   cfg.stream = st;
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = P::CL;
@@ -1993,7 +2122,10 @@ template <int V>
 inline int plane_clusters_of() {
   using P = PlaneVariant<V>;
   const void *fn = plane_fn<V>();
-  if (raise_smem(fn, plane_smem_of<P::CL, P::THREADS>()) != cudaSuccess) return 0;
+  if (raise_smem(fn, plane_smem_of<V>()) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
   if (P::CL > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
     cudaGetLastError();
     return 0;
@@ -2010,10 +2142,9 @@ inline int plane_clusters_of() {
 static inline int plane_clusters_per_device() { return plane_clusters_of<0>(); }
 template <int V>
 inline cudaError_t plane_launch(const SimDev &h, long long s, cudaStream_t st) {
-  using P = PlaneVariant<V>;
   cudaLaunchAttribute at[2];
   cudaLaunchConfig_t cfg = plane_cfg<V>(h.n1, st, at, true);
-  return cudaLaunchKernelEx(&cfg, k_plane_fast<PlaneFY, PlaneFZ, P::CL, P::THREADS, P::MINB>, h, s);
+  return cudaLaunchKernelEx(&cfg, plane_kernel<V>(), h, s);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -109,7 +109,7 @@ struct SimDev {
   int nonlinear;
   int dispersion;     // scalar c0 with :stokes absorption -> second spectrum
   int scalar_c;       // c^2 folded into M (scalar c0) vs applied per voxel
-  const float *M;     // [Nz][Ny][n1]
+  const float *M;     // [Nz][Ny][n1]; plane pass: [n1][Nz][slot] or slot-major [n1][slot][z]
   const float *M2;    // dispersion multiplier, [Nz][Ny][n1]
 
   const float *pml_def[3];
@@ -332,7 +332,12 @@ cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, lo
                       cudaStream_t st);
 bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
-int fast_plane_variants();
+int fast_plane_variants(int *ids = nullptr);
+// The chosen plane-pass variant wants its multiplier slot-major (fast_plane_relayout from the
+// [kx][k_z][slot] table).
+bool fast_plane_slot_major(const SimDev &h);
+cudaError_t fast_plane_prime();
+cudaError_t fast_plane_relayout(float *M, const float *M_kz_slot, int n1, cudaStream_t st);
 void fast_plane_slot_ky(int Ny, int *ky);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
 

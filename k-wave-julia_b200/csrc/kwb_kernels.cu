@@ -649,6 +649,7 @@ cudaError_t prime_attributes(const SimDev &h) {
   if (h.fast)
     for (int a = 0; a < h.ndim; ++a)
       if (fast_size(h.N[a]) && (e = fast_prime(h.N[a])) != cudaSuccess) return e;
+  if (h.plane && (e = fast_plane_prime()) != cudaSuccess) return e;
   return cudaSuccess;
 }
 

@@ -4,7 +4,8 @@
 // KWave.jl/src/fft_utils.jl:59-60).  Here every pass of the time step has a few valid schedules
 // and the fastest is measured on first use of a grid shape:
 //   * register-FFT passes: the tile variant -- full-width tiles, 128-thread tiles or one-warp
-//     tiles -- and, for the 3-D cluster plane pass, 8 CTAs of 512 threads or 16 of 256 per plane;
+//     tiles -- and, for the 3-D cluster plane pass, 8 CTAs of 512 threads or 16 of 256 per plane
+//     with row-major or slot-major rows;
 //   * Stockham passes (other lengths): the radix order of each axis's plan, the complex lines per
 //     tile, and the threads per CTA of the line passes.
 // Each candidate runs on the simulation's own buffers before its initial conditions are set
@@ -67,7 +68,7 @@ bool schedule_parse(const char *txt, Schedule &s) {
     return false;
   memset(&s, 0, sizeof(s));
   for (int i = 0; i < 8; ++i) {
-    if (tv[i] < -1 || tv[i] > 2) return false;
+    if (tv[i] < -1 || tv[i] > 3) return false;
     s.tile_var[i] = (signed char)tv[i];
   }
   for (int a = 0; a < 3; ++a) {
@@ -237,10 +238,14 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
     }
   }
 
-  // the 3-D cluster plane pass: 8 CTAs of 512 threads or 16 of 256 per kx plane
+  // the 3-D cluster plane pass: 8 CTAs of 512 threads or 16 of 256 per kx plane, rows kept
+  // row-major (block-wide z transforms) or slot-major (one warp per z line).  The slot-major
+  // kernels read the multiplier in another layout; timing them on the row-major table reads the
+  // same bytes from the same buffer.
   if (t.plane) {
-    const int nv = fast_plane_variants();
-    T.choose("plane", nv > 1 ? nv : 0, [&](int i) { t.tile_var[KWB_SLOT_PLANE] = (signed char)i; },
+    int ids[4];
+    const int nv = fast_plane_variants(ids);
+    T.choose("plane", nv > 1 ? nv : 0, [&](int i) { t.tile_var[KWB_SLOT_PLANE] = (signed char)ids[i]; },
              [&] { return fast_plane(d, t, 0, st); });
   }
   // spectrum passes along y and z
