@@ -710,6 +710,8 @@ size_t estimate_device_bytes(const kwb_problem *P) {
     // FP64 staging during set-up (released once the simulation is created)
     if (c_arr || r_arr || b_arr || P->p0.count)
       need += (size_t)nvox * 8 * (((nonlinear && b_arr && r_arr) ? 2 : 1) + ((P->row_major && D > 1) ? 1 : 0));
+    // the cluster plane pass's multiplier relayout copies the table once during set-up
+    if (D == 3 && fast_plane_size((int)N[1], (int)N[2])) need += (size_t)nspec * 4;
   }
   for (int g = 0; g < P->n_groups; ++g) {
     const kwb_sensor_group &G = P->groups[g];

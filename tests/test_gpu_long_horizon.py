@@ -53,6 +53,26 @@ def test_c2_full_horizon_against_fp64_golden(wl):
     print("c2 512^2 x 2000", rep)
 
 
+
+
+def test_c3_full_horizon_against_fp64_golden(wl):
+    """256^3, 1500 steps (the nonlinear absorbing workload the throughput is quoted on): the plane
+    p series at 1024 sampled points and the volume p_max at every 4th voxel against the FP64
+    oracle's run of all 1500 steps."""
+    gold = np.load(os.path.join(GOLDEN, "c3_long.npz"))
+    case = wl.c3()
+    assert int(gold["Nt"]) == case.Nt == 1500
+    case.sensor = dict(mask=_mask(case.N, gold["plane_idx"]), record=["p"])
+    case.extra_sensors = [dict(mask=_mask(case.N, gold["vol_idx"]), record=["p_max"])]
+    out = run_gpu(case)
+    rep = {}
+    for k, got, ref in (("p", out["p"], gold["p"]), ("p_max", out.extra[0]["p_max"], gold["p_max"])):
+        l2, mx = errors(got, ref.astype(np.float64))
+        rep[k] = (l2, mx)
+        assert l2 <= TOL_L2 and mx <= TOL_MAX, (k, l2, mx)
+    print("c3 256^3 x 1500", rep)
+
+
 def test_sampled_serving_requests_against_fp64_golden(wl):
     """Requests 0, 16 and 22 of the 48-request serving stream (two 2D, one 64^3), served together
     through the continuous-batching scheduler: each p series against the FP64 oracle's
