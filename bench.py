@@ -28,18 +28,18 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "k-wave-julia_b200"))
 
-# Spectral-pass-model words per voxel-step (algorithmic bytes = 4 B x words), per config.
-
 # DRAM bytes read + written (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# dominant kernel, averaged over the launches of one capture on a B200:
-#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum
-#       --clock-control none -k regex:'k_line_fast|k_plane_fast|k_eos_inv_fast' -s 60 -c 10
+# dominant kernel, from one capture on a B200 (the x line pass with the EOS operand prefetch and
+# the tuned 128-thread tiles; profiles/line_pass_x_eos_256cubed_ncu.md):
+#   ncu --set full --clock-control none --kernel-name-base demangled
+#       -k 'regex:k_line_fast<.*\(bool\)1, \(int\)[0-9]+, \(int\)2, \(bool\)1>' -s 14 -c 1
 #       python bench.py --steps 4 --warmup 3 --no-e2e --no-cpu --no-batch --no-serve --no-elastic
 #       --no-cufft --no-c2
 # Reads equal the algorithmic bytes; writes land lower because part of each launch's output is
 # still in L2 when the launch ends.
-NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 706.2e6}
+NCU_TRAFFIC = {("c3", "line_pass_x_eos_fwd"): 713.9e6}
 
+# Spectral-pass-model words per voxel-step (algorithmic bytes = 4 B x words), per config.
 SPM_WORDS = {"c3": 33.0, "c2": 26.0, "c1": 15.01}
 UNIT = "Gvoxel-steps/s"
 METRIC = "Gvoxel-steps/s (fluid k-space time stepping)"
