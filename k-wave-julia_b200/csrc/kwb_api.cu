@@ -1063,8 +1063,11 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   {
     const char *dc = getenv("KWB_TEST_DROP_TILE_COPY");
     h.test_drop_copy = dc && strcmp(dc, "1") == 0;
-    const char *tt = getenv("KWB_TILE_TMA");  // 0: contiguous tiles by 16-byte cp.async instead
-    h.tile_tma = !(tt && strcmp(tt, "0") == 0);
+    // line-pass tiles by TMA copies (1) or 16-byte cp.async (0, the default): the tuner measures
+    // both per pass unless KWB_TILE_TMA fixes the choice
+    const char *tt = getenv("KWB_TILE_TMA");
+    h.tile_tma = tt && strcmp(tt, "1") == 0;
+    memset(h.tma_line, -1, sizeof(h.tma_line));
     const char *ep = getenv("KWB_EOS_PREFETCH");  // 0: no L2 prefetch of the EOS operands
     h.eos_prefetch = !(ep && strcmp(ep, "0") == 0);
   }

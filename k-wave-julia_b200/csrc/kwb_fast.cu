@@ -2,6 +2,8 @@
 // instantiations and the entry points the launchers call.  The kernel templates live in
 // kwb_fast_impl.cuh; the mixed-radix lengths (3 * 2^k, 5 * 2^k) are instantiated in
 // kwb_fast_mixed.cu.
+#include <mutex>
+
 #include "kwb_fast_impl.cuh"
 
 namespace kwb {
@@ -83,6 +85,49 @@ cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaSt
     case 3: return fast::plane_launch<3>(h, s, st);
     default: return fast::plane_launch<0>(h, s, st);
   }
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once (the library links only the runtime).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+bool encode_strided_maps(SimDev &h, int axis, int cols) {
+  const EncodeTiledFn enc = encode_tiled_fn();
+  if (!enc || axis < 1 || axis > 2 || cols % 4 != 0 || h.N[0] % 4 != 0) return false;
+  const int N = h.N[axis];
+  int rows = 0;
+  for (int k = (N + 255) / 256; k <= N && !rows; ++k)
+    if (N % k == 0) rows = N / k;
+  // each box and the second staged tile start on 128-byte boundaries of shared memory
+  if (rows <= 0 || rows > 256 || (rows * cols * 4) % 128 != 0 || (N * cols * 4) % 128 != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)h.N[0], (cuuint64_t)h.N[1], (cuuint64_t)h.N[2]};
+  const cuuint64_t strides[2] = {(cuuint64_t)h.N[0] * 4, (cuuint64_t)h.N[0] * h.N[1] * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)(axis == 1 ? rows : 1), (cuuint32_t)(axis == 2 ? rows : 1)};
+  const cuuint32_t unit[3] = {1, 1, 1};
+  const float *fields[4] = {h.p, h.rho0, h.u[axis], h.rho[axis]};
+  for (int f = 0; f < 4; ++f) {
+    if (!fields[f]) continue;
+    if (enc(&h.tile_map[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(fields[f]), dims, strides, box,
+            unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  h.tile_box_rows = rows;
+  return true;
 }
 
 bool fast_size(int N) {

@@ -716,9 +716,11 @@ __device__ __forceinline__ void build_line_tables(float2 *tw, float2 *gp2, float
     gn2[q * RP + u] = gneg[k];
   }
 }
+// Register line pass: exchange buffers, twiddles and gradient tables, then the two staged operand
+// tiles, 128-byte aligned (destinations of tiled TMA copies).
 template <class F>
 __host__ __device__ constexpr size_t pline_offset(int L) {
-  return (((size_t)L * F::LP + F::TW + 2 * (size_t)F::E * (F::G + 1)) * sizeof(float2) + 15) & ~size_t(15);
+  return (((size_t)L * F::LP + F::TW + 2 * (size_t)F::E * (F::G + 1)) * sizeof(float2) + 127) & ~size_t(127);
 }
 template <class F>
 __host__ __device__ constexpr size_t pline_smem(int L) {
@@ -765,6 +767,17 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsign
                "l"(src), "r"(bytes), "r"(smem_u32(m))
                : "memory");
 }
+// Tiled tensor copy (TMA) of one box of a 3-D tensor map into shared memory, completing on the
+// mbarrier with the box's byte count.  The map lives in the kernel's parameter space; x is the
+// innermost coordinate (a multiple of 4 FP32 elements, 16 bytes); no multicast.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            unsigned long long *m) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(m))
+      : "memory");
+}
 // Bulk prefetch of a contiguous block into L2 (16-byte aligned address and size).
 __device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
@@ -794,34 +807,43 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *m, unsigne
 // XEOS (x axis, time steps only): the pass ends with the equation of state's x R2C for its tile,
 // as k_eos_fwd_fast does, starting from rho_x still in registers (rho_y and rho_z are final:
 // the x pass runs last).
-template <class F, bool CONTIG, int LT, int MINB, bool XEOS>
+// STMA (strided passes): the instantiation that can stage its tiles by tiled TMA copies; the
+// other one is the plain 16-byte cp.async pass.
+template <class F, bool CONTIG, int LT, int MINB, bool XEOS, bool STMA = false>
 __global__ void __launch_bounds__(LT * F::G, MINB)
     k_line_fast(const __grid_constant__ SimDev S, int axis, int mode, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int RP = G + 1, LP = F::LP;
   constexpr int L = LT;  // complex lines per tile
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
   float2 *gp2 = tw2 + F::TW;
   float2 *gn2 = gp2 + E * RP;
   // Contiguous tiles are 2L whole consecutive rows, so each field's tile is one block of
-  // memory: one bulk (TMA) copy per field, completing on its own mbarrier (0 p, 1 rho0,
-  // 2 u_d, 3 rho_d; each used for one phase).
+  // memory: one bulk (TMA) copy per field.  Strided tiles (2L columns of N rows) are boxes of
+  // the field's tensor map: N / tile_box_rows tiled TMA copies per field.  Each field's copies
+  // complete on its own mbarrier (0 p, 1 rho0, 2 u_d, 3 rho_d; each used for one phase).
+  // Tiled copies need 16-byte box rows and x offsets (2L a multiple of 4) and 128-byte aligned
+  // destinations (the staged tiles and each box within them; the host checks the box sizes).
+  constexpr bool TMA_S_OK = STMA && !CONTIG && (2 * LT) % 4 == 0;
+  const bool tma = CONTIG ? (S.tma_line[axis] >= 0 ? S.tma_line[axis] : S.tile_tma) != 0
+                          : (TMA_S_OK && S.tile_tma_s != 0 && S.tile_box_rows > 0 && F::N % S.tile_box_rows == 0 &&
+                             ((smem_u32(smem_raw) + (unsigned)pline_offset<F>(LT)) & 127u) == 0);
   __shared__ __align__(8) unsigned long long tile_bar[4];
-  if (CONTIG && threadIdx.x == 0) {
+  if (tma && threadIdx.x == 0) {
 #pragma unroll
     for (int b = 0; b < 4; ++b) mbar_init(&tile_bar[b], 1);
   }
   // the tables are written once at set-up: built before waiting on the previous kernel
   build_line_tables<F>(tw2, gp2, gn2, S.tw[axis], S.gpos[axis], S.gneg[axis]);
-  if (CONTIG) __syncthreads();  // the mbarriers are initialised for every thread
+  if (tma) __syncthreads();  // the mbarriers are initialised for every thread
   KWB_STEP_KERNEL_PROLOGUE();
   const long long t = *S.t0 + step_s;
   if (mode == KWB_MODE_STEP && t >= S.Nt) return;
   // once a wait has given up, the simulation is failed: later tiles exit at once instead of each
   // waiting out its budget (uniform over the CTA: one load before any thread diverges)
-  if (CONTIG && *reinterpret_cast<volatile const int *>(S.err) != 0) return;
+  if (tma && *reinterpret_cast<volatile const int *>(S.err) != 0) return;
   const int tid = threadIdx.x;
   const int tt = CONTIG ? tid % G : tid / L;
   const int l = CONTIG ? tid / G : tid % L;
@@ -883,13 +905,32 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // thread's chunks differ by constants.
   auto stage = [&](float *dst, const float *f, int slot) {
     const float *fb = f + base;
-    if (CONTIG && S.tile_tma) {
+    if (CONTIG && tma) {
       // rows contiguous in memory: one bulk copy of cnt rows (16-byte aligned: N % 4 == 0)
       if (tid == 0) {
         const unsigned bytes = (unsigned)cnt * N * 4u;
         fence_proxy_async_smem();
         mbar_expect_tx(&tile_bar[slot], bytes);
         if (!(S.test_drop_copy && slot == 0 && blockIdx.x == 0)) bulk_copy_g2s(dst, fb, bytes, &tile_bar[slot]);
+      }
+      return;
+    } else if (!CONTIG && tma) {
+      // the tile is a box of the field's tensor map, N / BR boxes of BR positions: columns past
+      // the grid edge arrive as zeros (the map's out-of-bounds fill)
+      if (tid == 0) {
+        // the tile's first column and its fixed (z or y) index, recomputed here rather than kept
+        // live through the transforms
+        const int tpp = (Nx + 2 * L - 1) / (2 * L);
+        const int to = blockIdx.x / tpp, tx0 = (blockIdx.x - to * tpp) * 2 * L;
+        const int BR = S.tile_box_rows;
+        fence_proxy_async_smem();
+        mbar_expect_tx(&tile_bar[slot], (unsigned)(2 * L * N * 4));
+        if (!(S.test_drop_copy && slot == 0 && blockIdx.x == 0)) {
+          for (int c = 0; c * BR < N; ++c) {
+            if (axis == 1) tma_load_3d(dst + c * BR * 2 * L, &S.tile_map[slot], tx0, c * BR, to, &tile_bar[slot]);
+            else tma_load_3d(dst + c * BR * 2 * L, &S.tile_map[slot], tx0, to, c * BR, &tile_bar[slot]);
+          }
+        }
       }
       return;
     } else if (CONTIG) {
@@ -920,7 +961,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   // any copy still in flight before the CTA exits.
   bool issued[4] = {false, false, false, false};
   auto tile_wait = [&](int s0, int s1) -> bool {
-    if (!S.tile_tma) {  // 16-byte cp.async staging: the p tile alone first, then everything
+    if (!tma) {  // 16-byte cp.async staging: the p tile alone first, then everything
       if (s0 == 0 && s1 < 0) cp_async_wait<1>();
       else cp_async_wait<0>();
       __syncthreads();
@@ -947,17 +988,13 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   if (rho0) {
     stage(st_r, rho0, 1);
     issued[1] = true;
-  } else if (!CONTIG || !S.tile_tma) {
+  } else if (!tma) {
     cp_async_commit();
   }
   float2 *xs = sm + l * LP;
   float *__restrict__ ud = S.u[axis];
-  if constexpr (CONTIG) {
-    if (!tile_wait(0, -1)) return;  // the p tile has landed (rho0 may still be in flight)
-  } else {
-    cp_async_wait<1>();  // the p tile has landed (rho0 may still be in flight)
-    __syncthreads();     // ... for every thread; tables too
-  }
+  // the p tile has landed (rho0 may still be in flight), for every thread; tables too
+  if (!tile_wait(0, -1)) return;
   float2 v[E];
 #pragma unroll
   for (int r = 0; r < E; ++r) v[r] = staged(st_p, tt + G * r);
@@ -974,12 +1011,8 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
 #pragma unroll
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gp2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
-  if constexpr (CONTIG) {
-    if (!tile_wait(rho0 ? 1 : -1, mode == KWB_MODE_STEP ? 2 : -1)) return;
-  } else {
-    cp_async_wait<0>();
-    __syncthreads();  // the rho0 and velocity tiles have landed
-  }
+  // the rho0 and velocity tiles have landed
+  if (!tile_wait(rho0 ? 1 : -1, mode == KWB_MODE_STEP ? 2 : -1)) return;
 
   // velocity update u = pml_sg (pml_sg u - dt/rho_sg dp)
   const float *__restrict__ esg = S.pml_sg_def[axis];
@@ -1069,12 +1102,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   for (int q = 0; q < E; ++q) v[q] = cmul(v[q], gn2[q * RP + tt]);
   F::inv(v, xs, tw2, tt);
 
-  if constexpr (CONTIG) {
-    if (!tile_wait(3, -1)) return;  // the rho_d tile has landed
-  } else {
-    cp_async_wait<0>();
-    __syncthreads();  // the rho_d tile has landed
-  }
+  if (!tile_wait(3, -1)) return;  // the rho_d tile has landed
   // density update rho_d = pml (pml rho_d - dt rho0 du)
   const float *__restrict__ ed = S.pml_def[axis];
 #pragma unroll
@@ -1190,7 +1218,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_fwd_fast(const __grid_constant__ SimDev S, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
   // the twiddles are written once at set-up: built before waiting on the previous kernel
@@ -1280,7 +1308,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     k_eos_inv_fast(const __grid_constant__ SimDev S, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, N = E * G, L = LT;
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
   // the twiddles are written once at set-up: built before waiting on the previous kernel
@@ -1440,7 +1468,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
     k_spec_fast(const __grid_constant__ SimDev S, int axis, int op, long long step_s) {
   constexpr int E = F::E, G = F::G;
   constexpr int LP = F::LP, L = LT;
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
   // the twiddles are written once at set-up: built before waiting on the previous kernel
@@ -1553,7 +1581,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   constexpr int LY = THREADS / FY::G, LZ = THREADS / FZ::G;
   static_assert(RZ == 2 * LY && CY % LZ == 0 && NZ % RZ == 0, "plane tiling");
   constexpr int XS = (LY * FY::LP > LZ * FZ::LP) ? LY * FY::LP : LZ * FZ::LP;
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *data = reinterpret_cast<float2 *>(smem_raw);  // [RZ][NY]
   float2 *xsb = data + RZ * NY;
   float2 *twy = xsb + XS;
@@ -1672,7 +1700,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
   constexpr int RP = RZ + 1;  // pitch of a slot column (odd: conflict-free row stores)
   static_assert(F::G == 32 && F::WARP_SYNC, "one warp per line");
   static_assert(RZ % W == 0 && CY % W == 0 && NZ % RZ == 0, "plane tiling");
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *cols = reinterpret_cast<float2 *>(smem_raw);  // [NY][RP]
   float2 *xsb = cols + NY * RP;                          // one exchange buffer per warp
   float2 *twy = xsb + W * F::LP;
@@ -1920,6 +1948,8 @@ static inline cudaError_t prime_line_variant() {
   if (e == cudaSuccess) e = raise_smem((const void *)k_el_grad_fast<F, C, LT, P::MINB>, pline_smem<F>(LT));
   if constexpr (C) {
     if (e == cudaSuccess) e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, true>, pline_smem<F>(LT));
+  } else {
+    if (e == cudaSuccess) e = raise_smem((const void *)k_line_fast<F, C, LT, P::MINB, false, true>, pline_smem<F>(LT));
   }
   return e;
 }
@@ -1951,7 +1981,19 @@ static inline void line_go(const SimDev *d_sim, const SimDev &h, int axis, int m
       kwb_launch(k_line_fast<F, true, LT, P::MINB, false>, grid, LT * F::G, pline_smem<F>(LT), st, h, axis, mode, s);
   } else {
     using F = typename P::template F<false>;
-    kwb_launch(k_line_fast<F, false, LT, P::MINB, false>, cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]), LT * F::G, pline_smem<F>(LT), st, h, axis, mode, s);
+    const int grid = cdiv(h.N[0], 2 * LT) * (axis == 1 ? h.N[2] : h.N[1]);
+    const bool want = (h.tma_line[axis] >= 0 ? h.tma_line[axis] : h.tile_tma) != 0;
+    if (want && (2 * LT) % 4 == 0) {
+      // strided tiles by tiled TMA: this launch's copy of the descriptor carries the fields'
+      // tensor maps for its tile width (16-byte rows and offsets only)
+      SimDev hs = h;
+      if (encode_strided_maps(hs, axis, 2 * LT)) {
+        hs.tile_tma_s = 1;
+        kwb_launch(k_line_fast<F, false, LT, P::MINB, false, true>, grid, LT * F::G, pline_smem<F>(LT), st, hs, axis, mode, s);
+        return;
+      }
+    }
+    kwb_launch(k_line_fast<F, false, LT, P::MINB, false>, grid, LT * F::G, pline_smem<F>(LT), st, h, axis, mode, s);
   }
 }
 
@@ -2161,7 +2203,7 @@ __global__ void __launch_bounds__(LT * F::G, MINB)
   constexpr int E = F::E, G = F::G;
   constexpr int RP = G + 1, LP = F::LP;
   constexpr int L = LT;
-  extern __shared__ float4 smem_raw[];
+  extern __shared__ __align__(128) float4 smem_raw[];
   float2 *sm = reinterpret_cast<float2 *>(smem_raw);
   float2 *tw2 = sm + L * LP;
   float2 *gp2 = tw2 + F::TW;

@@ -12,6 +12,7 @@
 #pragma once
 #include <string>
 #include <utility>
+#include <cuda.h>  // CUtensorMap (the tensor-map type only; the encoder is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -170,7 +171,11 @@ struct SimDev {
   // complete); the host reads it after synchronising and reports KWB_E_DEVICE.
   int *err;
   int test_drop_copy;  // test hook: the first CTA of a contiguous line pass drops its p-tile copy
-  int tile_tma;        // contiguous line-pass tiles by bulk TMA copies (1) or 16-byte cp.async (0)
+  // Register line passes: tiles staged by TMA copies (1: bulk copies of contiguous rows, tiled
+  // tensor copies of strided columns) or by 16-byte cp.async (0); tma_line[axis] is the measured
+  // choice of each pass (-1: tile_tma, the default).
+  int tile_tma;
+  signed char tma_line[3];
   int eos_prefetch;    // the fused x pass prefetches its equation-of-state operands into L2
   int num_sms;        // multiprocessors of the device (tile sizing)
   int tile_override;  // register-FFT tile variant forced for every pass (-1: chosen per pass)
@@ -199,6 +204,13 @@ struct SimDev {
   const float *s_sig[6];        // stress source tables [col][j]; nullptr when a component is absent
   const long long *s_idx;       // stress source points (column-major linear indices)
   const long long *u_idx;       // velocity source points (elastic solver)
+
+  // Strided (y / z) register line passes: tensor maps of the staged fields (0 p, 1 rho0, 2 u_d,
+  // 3 rho_d), each box 2L columns x tile_box_rows positions along the line, encoded by the host
+  // for the launch that uses them (fast_line_pass); tile_tma_s = 0 stages by 16-byte cp.async.
+  int tile_tma_s;
+  int tile_box_rows;
+  alignas(64) CUtensorMap tile_map[4];
 };
 
 // Stress slot of sigma_{dj}: the diagonal in 0..2, the pair {d, j} in 3..5 (xy, xz, yz).
@@ -337,6 +349,11 @@ int fast_plane_variants(int *ids = nullptr);
 // [kx][k_z][slot] table).
 bool fast_plane_slot_major(const SimDev &h);
 cudaError_t fast_plane_prime();
+// Tensor maps of the fields a strided register line pass stages (p, rho0, u_d, rho_d), boxes of
+// `cols` columns x N / k positions along `axis` (the smallest k with N / k <= 256 dividing N);
+// false when the driver's encoder is unavailable or rejects a map (the pass then stages by
+// 16-byte cp.async).
+bool encode_strided_maps(SimDev &h, int axis, int cols);
 cudaError_t fast_plane_relayout(float *M, const float *M_kz_slot, int n1, cudaStream_t st);
 void fast_plane_slot_ky(int Ny, int *ky);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
@@ -373,6 +390,7 @@ cudaError_t filter_apply(float *out, const float *in, const float *h, const int 
 // FFT schedule (kwb_tune.cu): the tuned fields of a SimDev.
 struct Schedule {
   signed char tile_var[8];
+  signed char tma_line[3];
   short thr_line[3];
   int L_line[3], L_eosx, L_spec[3];
   signed char plan_order[3];

@@ -4,7 +4,8 @@
 // KWave.jl/src/fft_utils.jl:59-60).  Here every pass of the time step has a few valid schedules
 // and the fastest is measured on first use of a grid shape:
 //   * register-FFT passes: the tile variant -- full-width tiles, 128-thread tiles or one-warp
-//     tiles -- and, for the 3-D cluster plane pass, 8 CTAs of 512 threads or 16 of 256 per plane
+//     tiles --, for the line passes whether the tiles are staged by TMA copies or by 16-byte
+//     cp.async, and, for the 3-D cluster plane pass, 8 CTAs of 512 threads or 16 of 256 per plane
 //     with row-major or slot-major rows;
 //   * Stockham passes (other lengths): the radix order of each axis's plan, the complex lines per
 //     tile, and the threads per CTA of the line passes.
@@ -18,6 +19,7 @@
 // only on request (KWB_TUNE_ORDER=1), since it gives up that bit-for-bit agreement.
 #include <cfloat>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -29,6 +31,7 @@ namespace kwb {
 void schedule_of(const SimDev &h, Schedule &s) {
   memset(&s, 0, sizeof(s));
   memcpy(s.tile_var, h.tile_var, sizeof(s.tile_var));
+  memcpy(s.tma_line, h.tma_line, sizeof(s.tma_line));
   for (int a = 0; a < 3; ++a) {
     s.thr_line[a] = h.thr_line[a];
     s.L_line[a] = h.L_line[a];
@@ -40,6 +43,7 @@ void schedule_of(const SimDev &h, Schedule &s) {
 
 void schedule_apply(SimDev &h, const Schedule &s) {
   memcpy(h.tile_var, s.tile_var, sizeof(h.tile_var));
+  memcpy(h.tma_line, s.tma_line, sizeof(h.tma_line));
   for (int a = 0; a < 3; ++a) {
     h.thr_line[a] = s.thr_line[a];
     h.L_line[a] = s.L_line[a];
@@ -52,21 +56,26 @@ void schedule_apply(SimDev &h, const Schedule &s) {
 
 std::string schedule_str(const Schedule &s) {
   char buf[256];
-  snprintf(buf, sizeof(buf), "tile=%d,%d,%d,%d,%d,%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d",
+  snprintf(buf, sizeof(buf),
+           "tile=%d,%d,%d,%d,%d,%d,%d,%d tma=%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d",
            s.tile_var[0], s.tile_var[1], s.tile_var[2], s.tile_var[3], s.tile_var[4], s.tile_var[5],
-           s.tile_var[6], s.tile_var[7], s.thr_line[0], s.thr_line[1], s.thr_line[2], s.L_line[0], s.L_line[1],
-           s.L_line[2], s.L_eosx, s.L_spec[1], s.L_spec[2], s.plan_order[0], s.plan_order[1],
-           s.plan_order[2]);
+           s.tile_var[6], s.tile_var[7], s.tma_line[0], s.tma_line[1], s.tma_line[2], s.thr_line[0], s.thr_line[1],
+           s.thr_line[2], s.L_line[0], s.L_line[1], s.L_line[2], s.L_eosx, s.L_spec[1], s.L_spec[2],
+           s.plan_order[0], s.plan_order[1], s.plan_order[2]);
   return buf;
 }
 
 bool schedule_parse(const char *txt, Schedule &s) {
-  int tv[8], th[3], L[6], po[3];
-  if (sscanf(txt, "tile=%d,%d,%d,%d,%d,%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d", &tv[0],
-             &tv[1], &tv[2], &tv[3], &tv[4], &tv[5], &tv[6], &tv[7], &th[0], &th[1], &th[2], &L[0], &L[1],
-             &L[2], &L[3], &L[4], &L[5], &po[0], &po[1], &po[2]) != 20)
+  int tv[8], tm[3], th[3], L[6], po[3];
+  if (sscanf(txt, "tile=%d,%d,%d,%d,%d,%d,%d,%d tma=%d,%d,%d threads=%d,%d,%d L=%d,%d,%d,%d,%d,%d order=%d,%d,%d",
+             &tv[0], &tv[1], &tv[2], &tv[3], &tv[4], &tv[5], &tv[6], &tv[7], &tm[0], &tm[1], &tm[2], &th[0], &th[1],
+             &th[2], &L[0], &L[1], &L[2], &L[3], &L[4], &L[5], &po[0], &po[1], &po[2]) != 23)
     return false;
   memset(&s, 0, sizeof(s));
+  for (int a = 0; a < 3; ++a) {
+    if (tm[a] < -1 || tm[a] > 1) return false;
+    s.tma_line[a] = (signed char)tm[a];
+  }
   for (int i = 0; i < 8; ++i) {
     if (tv[i] < -1 || tv[i] > 3) return false;
     s.tile_var[i] = (signed char)tv[i];
@@ -195,6 +204,9 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
     auto go = [&, a] { return launch_line_pass(d, t, a, KWB_MODE_STEP, 0, st); };
     if (line_is_fast(t, a)) {
       T.choose("line_tile", 3, [&, a](int i) { t.tile_var[KWB_SLOT_LINE0 + a] = (signed char)i; }, go);
+      // tiles staged by TMA copies or by 16-byte cp.async (unless KWB_TILE_TMA fixes it)
+      if (!getenv("KWB_TILE_TMA"))
+        T.choose("line_tma", 2, [&, a](int i) { t.tma_line[a] = (signed char)(i == 0 ? 0 : 1); }, go);
       continue;
     }
     // Stockham: radix order (distinct plans only; with explore_order), then lines per tile,

@@ -368,11 +368,30 @@ def test_bluestein_lengths(kb, shape):
     assert_parity(run_gpu(case), run_oracle(case), TOL_L2, TOL_MAX)
 
 
+@pytest.mark.parametrize("shape", [(512, 512), (1024, 256), (256, 1024), (64, 64, 64), (96, 80, 160), (256, 500)])
+def test_tiled_tma_staging_matches_cp_async(kb, monkeypatch, shape):
+    """The strided (y / z) line passes stage their tiles with tiled TMA copies of the fields'
+    tensor maps (boxes of 2L columns x up to 256 positions; lines of 512 and 1024 take 2 and 4
+    boxes; columns past the grid edge come back as zeros), the contiguous passes with bulk copies.
+    Fields are bit-identical to 16-byte cp.async staging (KWB_TILE_TMA=0).  Lines whose boxes
+    would not start on 128-byte boundaries (500 = 2 x 250 with 4-column tiles) keep cp.async."""
+    monkeypatch.setenv("KWB_TUNE", "0")
+    case = _p0_case(shape, sum(shape), Nt=12, pml=8 if len(shape) == 2 else 6)
+    out = {}
+    for tma in ("1", "0"):
+        monkeypatch.setenv("KWB_TILE_TMA", tma)
+        out[tma] = run_gpu(case)
+    assert set(out["1"].data) == set(out["0"].data) == {"p_final", "p_max", "p_rms"}
+    for k in out["0"].data:
+        assert np.array_equal(np.asarray(out["1"][k]), np.asarray(out["0"][k])), (shape, k)
+
+
 def test_bounded_tile_wait_reports_an_error(kb, monkeypatch):
-    """The contiguous line pass stages its tiles with bulk (TMA) copies completing on mbarriers;
-    every wait is bounded by a clock budget.  With the test hook the first CTA's p-tile copy is
-    never issued, so its wait runs out (about half a second): the kernel sets the device error
-    word and returns, the host reports KWB_E_DEVICE, and the context keeps working."""
+    """The line passes stage their tiles with TMA copies (bulk copies of contiguous rows, tiled
+    tensor copies of strided columns) completing on mbarriers; every wait is bounded by a clock
+    budget.  With the test hook the first CTA's p-tile copy is never issued, so its wait runs out
+    (about half a second): the kernel sets the device error word and returns, the host reports
+    KWB_E_DEVICE, and the context keeps working."""
     from kwave_b200.workloads import c2
     monkeypatch.setenv("KWB_TUNE", "0")
     monkeypatch.setenv("KWB_TILE_TMA", "1")
