@@ -17,7 +17,7 @@ bool fast_plane_available() {
 // Plane-pass variants usable on this device, in the order the tuner tries them (their ids in
 // ids[]; 16-CTA clusters need the non-portable cluster size).
 int fast_plane_variants(int *ids) {
-  static int n = -1, v[4];
+  static int n = -1, v[KWB_PLANE_VARIANTS];
   if (n < 0) {
     int k = 0;
     if (fast_plane_available()) {
@@ -25,6 +25,8 @@ int fast_plane_variants(int *ids) {
       if (fast::plane_clusters_of<2>() > 0) v[k++] = 2;
       if (fast::plane_clusters_of<1>() > 0) v[k++] = 1;
       if (fast::plane_clusters_of<3>() > 0) v[k++] = 3;
+      if (fast::plane_clusters_of<4>() > 0) v[k++] = 4;
+      if (fast::plane_clusters_of<5>() > 0) v[k++] = 5;
     }
     n = k;
   }
@@ -35,7 +37,7 @@ int fast_plane_variants(int *ids) {
 // The variant a simulation runs: its measured choice, else slot-major 8 x 512 (108 vs 112 µs per
 // 256^3 launch for row-major 8 x 512, 117 and 127 µs for the 16-CTA shapes), else row-major.
 static int plane_variant_of(const SimDev &h) {
-  int ids[4];
+  int ids[KWB_PLANE_VARIANTS];
   const int n = fast_plane_variants(ids);
   const int want = h.tile_var[KWB_SLOT_PLANE] >= 0 ? h.tile_var[KWB_SLOT_PLANE] : 2;
   for (int i = 0; i < n; ++i)
@@ -53,7 +55,7 @@ static cudaError_t plane_prime_one() {
   return e;
 }
 cudaError_t fast_plane_prime() {
-  int ids[4];
+  int ids[KWB_PLANE_VARIANTS];
   const int n = fast_plane_variants(ids);
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < n && e == cudaSuccess; ++i) {
@@ -61,6 +63,8 @@ cudaError_t fast_plane_prime() {
       case 1: e = plane_prime_one<1>(); break;
       case 2: e = plane_prime_one<2>(); break;
       case 3: e = plane_prime_one<3>(); break;
+      case 4: e = plane_prime_one<4>(); break;
+      case 5: e = plane_prime_one<5>(); break;
       default: e = plane_prime_one<0>(); break;
     }
   }
@@ -83,6 +87,8 @@ cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaSt
     case 1: return fast::plane_launch<1>(h, s, st);
     case 2: return fast::plane_launch<2>(h, s, st);
     case 3: return fast::plane_launch<3>(h, s, st);
+    case 4: return fast::plane_launch<4>(h, s, st);
+    case 5: return fast::plane_launch<5>(h, s, st);
     default: return fast::plane_launch<0>(h, s, st);
   }
 }

@@ -2097,7 +2097,8 @@ static inline cudaError_t launch_spec_n(const SimDev *d_sim, const SimDev &h, in
 // Cluster plane pass for Ny = Nz = 256.  Variants: 0 -- k_plane_fast with 8 CTAs of 512 threads
 // per kx plane (32 rows each); 1 -- k_plane_fast with 16 CTAs of 256 threads (16 rows each; a
 // non-portable cluster size); 2 and 3 -- k_plane_cols with the same two cluster shapes (its
-// multiplier in the slot-major layout).
+// multiplier in the slot-major layout); 4 and 5 -- k_plane_cols with 1024-thread CTAs in
+// clusters of 4 or 8.
 using PlaneFY = LinePolicy<256>::F<true>;
 using PlaneFZ = LinePolicy<256>::F<false>;
 template <int V> struct PlaneVariant;
@@ -2115,6 +2116,15 @@ template <> struct PlaneVariant<2> {
 };
 template <> struct PlaneVariant<3> {
   static constexpr int CL = 16, THREADS = 256, MINB = 3;
+  static constexpr bool COLS = true;
+};
+// one 1024-thread CTA per SM: clusters of 4 (64 rows each) or of 8 (32 rows, one per warp)
+template <> struct PlaneVariant<4> {
+  static constexpr int CL = 4, THREADS = 1024, MINB = 1;
+  static constexpr bool COLS = true;
+};
+template <> struct PlaneVariant<5> {
+  static constexpr int CL = 8, THREADS = 1024, MINB = 1;
   static constexpr bool COLS = true;
 };
 template <int V>

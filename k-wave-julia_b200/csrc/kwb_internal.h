@@ -344,6 +344,7 @@ cudaError_t fast_spec(const SimDev *d_sim, const SimDev &h, int axis, int op, lo
                       cudaStream_t st);
 bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
+#define KWB_PLANE_VARIANTS 6  // cluster plane-pass variants (kwb_fast_impl.cuh PlaneVariant)
 int fast_plane_variants(int *ids = nullptr);
 // The chosen plane-pass variant wants its multiplier slot-major (fast_plane_relayout from the
 // [kx][k_z][slot] table).

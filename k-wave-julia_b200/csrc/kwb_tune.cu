@@ -77,7 +77,7 @@ bool schedule_parse(const char *txt, Schedule &s) {
     s.tma_line[a] = (signed char)tm[a];
   }
   for (int i = 0; i < 8; ++i) {
-    if (tv[i] < -1 || tv[i] > 3) return false;
+    if (tv[i] < -1 || tv[i] >= KWB_PLANE_VARIANTS) return false;
     s.tile_var[i] = (signed char)tv[i];
   }
   for (int a = 0; a < 3; ++a) {
@@ -255,7 +255,7 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
   // kernels read the multiplier in another layout; timing them on the row-major table reads the
   // same bytes from the same buffer.
   if (t.plane) {
-    int ids[4];
+    int ids[KWB_PLANE_VARIANTS];
     const int nv = fast_plane_variants(ids);
     T.choose("plane", nv > 1 ? nv : 0, [&](int i) { t.tile_var[KWB_SLOT_PLANE] = (signed char)ids[i]; },
              [&] { return fast_plane(d, t, 0, st); });

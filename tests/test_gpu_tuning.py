@@ -56,15 +56,15 @@ def _fields(out):
 @pytest.mark.parametrize("name", ["stockham_2d_270", "register_2d_256", "stockham_3d_48", "stockham_3d_96",
                                   "plane_3d_256"])
 def test_every_candidate_gives_the_same_fields(kb, name, monkeypatch):
-    """Candidates 0..3 of every pass (tile variants, lines per tile, threads per CTA, the plane
-    pass's cluster shape): fields bit-identical to the size heuristic's; the radix orders
-    explored with KWB_TUNE_ORDER=1 agree to FP32 rounding."""
+    """Candidates 0..5 of every pass (tile variants, TMA or cp.async staging, lines per tile,
+    threads per CTA, the plane pass's six variants): fields bit-identical to the size heuristic's;
+    the radix orders explored with KWB_TUNE_ORDER=1 agree to FP32 rounding."""
     case = _cases()[name]
     monkeypatch.setenv("KWB_TUNE", "0")
     ref, sched = _run(kb, case)
     assert sched.startswith("heuristic"), sched
     monkeypatch.delenv("KWB_TUNE")
-    for pick in range(4):
+    for pick in range(6 if name == "plane_3d_256" else 4):
         monkeypatch.setenv("KWB_TUNE_PICK", str(pick))
         out, sched = _run(kb, case)
         assert sched.startswith(f"pick {pick}"), sched
