@@ -553,8 +553,7 @@ def main():
     if not args.no_e2e:
         t0 = time.perf_counter()
         sim2 = kb.Simulation(g, m, s, sen, extra_sensors=case.extra_sensors, context=ctx, **kw)
-        sim2.advance(case.Nt)
-        out = sim2.outputs()
+        out = sim2.finish()
         el = time.perf_counter() - t0
         sim2.close()
         h2d = sum(np.asarray(v).nbytes for v in (case.medium["sound_speed"], case.medium["density"],

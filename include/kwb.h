@@ -221,6 +221,13 @@ int kwb_sim_sync(kwb_sim *sim);
 /* Finalize (p_rms/u_rms square roots, directivity-free outputs) and copy all recorded outputs
  * to the caller's FP64 buffers.  Blocks. */
 int kwb_sim_read_outputs(kwb_sim *sim, kwb_outputs *outputs);
+/* Run the remaining steps and read all outputs (kwb_sim_advance to Nt, then
+ * kwb_sim_read_outputs), copying the recorded time series to the caller's buffers block by
+ * block while later steps run, so that only the last block's rows and the aggregates are read
+ * after the loop.  kwb_solve is kwb_sim_create + kwb_sim_finish + kwb_sim_destroy.  Blocks.
+ * (No reference counterpart of its own: the reference's loop returns its outputs at the end,
+ * KWave.jl/src/solver/first_order.jl:448-484.) */
+int kwb_sim_finish(kwb_sim *sim, kwb_outputs *outputs);
 /* Copy the current FP32 pressure field (N voxels, column-major) to host memory.  Blocks. */
 int kwb_sim_read_pressure(kwb_sim *sim, float *p_host);
 void kwb_sim_destroy(kwb_sim *sim);

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -923,6 +924,36 @@ static int choose_schedule(kwb_sim *S, SimDev &h, cudaStream_t st) {
   return KWB_OK;
 }
 
+// Set-up phase times (KWB_SETUP_LOG=1): the stream is synchronised at each mark, so the figures
+// include the device work each phase queued; a diagnostic, printed to stderr.
+struct SetupLog {
+  bool on = false;
+  cudaStream_t st = nullptr;
+  std::chrono::steady_clock::time_point t0, last;
+  std::string line;
+  void start(cudaStream_t s) {
+    const char *e = getenv("KWB_SETUP_LOG");
+    on = e && strcmp(e, "1") == 0;
+    st = s;
+    t0 = last = std::chrono::steady_clock::now();
+  }
+  void mark(const char *what) {
+    if (!on) return;
+    cudaStreamSynchronize(st);
+    const auto now = std::chrono::steady_clock::now();
+    char b[96];
+    snprintf(b, sizeof(b), "%s %.1f ", what, std::chrono::duration<double, std::milli>(now - last).count());
+    line += b;
+    last = now;
+  }
+  void done() {
+    if (!on) return;
+    mark("rest");
+    fprintf(stderr, "kwb setup ms: %stotal %.1f\n", line.c_str(),
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+};
+
 int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   if (!ctx || !out) return KWB_E_INVALID;
   *out = nullptr;
@@ -948,6 +979,8 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   cudaStream_t st = S->stream;
   SimDev &h = S->h;
   DevBuf &M = S->mem;
+  SetupLog slog;
+  slog.start(st);
 
   const int D = P->ndim;
   h.ndim = D;
@@ -1057,6 +1090,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
                      need / 1e6, free_b / 1e6);
   }
 
+  slog.mark("admission");
   // ---- fields
   CU(M.alloc(&h.err, 1));
   CU(cudaMemsetAsync(h.err, 0, sizeof(int), st));
@@ -1099,6 +1133,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   CU(cudaMemsetAsync(S->d_t0, 0, 8, st));
   h.t0 = S->d_t0;
 
+  slog.mark("fields");
   // ---- medium (FP64 upload, FP32 on device); the FP64 staging is set-up scratch only
   TempBuf tmp(st, ctx->pool);
   double *stage = nullptr, *stage2 = nullptr, *rm_in = nullptr;
@@ -1199,6 +1234,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
 
   }
 
+  slog.mark("medium");
   // ---- per-axis tables (FP64 on device)
   for (int a = 0; a < 3; ++a) {
     const int n = h.N[a];
@@ -1276,6 +1312,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     h.M2 = M2;
   }
 
+  slog.mark("tables");
   // ---- sources
   auto c_at_points = [&](const int64_t *idx, long long n, double **dev_out) -> int {
     *dev_out = nullptr;
@@ -1386,6 +1423,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     CU(cudaStreamSynchronize(st));
   }
 
+  slog.mark("sources");
   // ---- sensor groups
   S->groups.resize(P->n_groups);
   // Pressure-only groups can be recorded by the fast x C2R pass as it writes p: one dense group
@@ -1481,6 +1519,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if (G.fused) h.sparse_p = G.d_dev;
   }
 
+  slog.mark("sensors");
   // ---- time reversal data: p / (D c^2) at group 0's points
   if (S->tr) {
     const kwb_sensor_group &G0 = P->groups[0];
@@ -1522,6 +1561,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   }
   CU(h.elastic ? el_prime(h) : prime_attributes(h));
 
+  slog.mark("tr+dense");
   // ---- FFT schedule: measured on first use of this shape (simulations of the batching
   // scheduler share the GPU with others, so they keep the heuristic)
   if (!h.elastic && !ctx->batched && S->Nt_loop > 0) {
@@ -1537,10 +1577,12 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     CU(fast_plane_relayout(const_cast<float *>(h.M), Mk, h.n1, st));
   }
 
+  slog.mark("schedule");
   // ---- device descriptor
   CU(M.alloc(&S->d_sim, 1));
   if ((rc = upload(ctx, S->d_sim, &h, sizeof(SimDev), st))) return rc;
 
+  slog.mark("descriptor");
   // ---- p0 initialisation (first_order_steps.jl:58-191); skipped in time-reversal mode
   if (P->p0.count && !S->tr) {
     if ((rc = upload_grid(stage, P->p0.data))) return rc;
@@ -1557,6 +1599,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   S->progress_user = P->progress_user;
   if (S->progress) CU(cudaMallocHost(&S->p_host, nvox * 4));
   S->launches_per_step = count_launches(S.get());
+  slog.done();
   *out = S.release();
   return KWB_OK;
 }
@@ -1581,6 +1624,12 @@ static int sim_enqueue(kwb_sim *S, long long steps) {
   if (steps >= KWB_CHUNK_STEPS && !S->graph) {
     const int rc = build_chunk_graph(S);
     if (rc) return rc;
+  }
+  // steps launched one by one index from the device counter t0 (step_s = steps_done - t0_host);
+  // a graph chunk indexes from t0 itself, so t0 first catches up with them
+  if (S->graph && steps >= S->graph_K && S->t0_host != S->steps_done) {
+    CU(launch_advance_t0(S->d_t0, S->steps_done - S->t0_host, S->stream));
+    S->t0_host = S->steps_done;
   }
   while (S->graph && steps >= S->graph_K) {
     CU(cudaGraphLaunch(S->graph, S->stream));
@@ -1685,7 +1734,11 @@ static int apply_post_filters(kwb_sim *S, GroupHost &G) {
   return KWB_OK;
 }
 
-int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
+}  // extern "C"
+
+// Read a simulation's outputs into the caller's arrays; the first row0 time rows of every time
+// series are already there (kwb_solve streams them while later steps run).
+static int read_outputs_from(kwb_sim *S, kwb_outputs *out, long long row0) {
   if (!S || !out) return KWB_E_INVALID;
   kwb_ctx *ctx = S->ctx;
   CU(cudaSetDevice(ctx->device));
@@ -1728,9 +1781,11 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
     };
     int rc;
     if (want(KWB_REC_P) && !G.filt_sin.empty() && (rc = apply_post_filters(S, S->groups[g]))) return rc;
-    if (want(KWB_REC_P) && (rc = get32(gd.ser_p, n * gd.nt_alloc, o.field[KWB_REC_P]))) return rc;
+    const long long r0 = std::min(row0, gd.nt_alloc), rows = gd.nt_alloc - r0;
+    if (want(KWB_REC_P) && (rc = get32(gd.ser_p + r0 * n, n * rows, o.field[KWB_REC_P] + r0 * n))) return rc;
     for (int d = 0; d < 3; ++d)
-      if (want(KWB_REC_UX + d) && (rc = get32(gd.ser_u[d], n * gd.nt_alloc, o.field[KWB_REC_UX + d]))) return rc;
+      if (want(KWB_REC_UX + d) && (rc = get32(gd.ser_u[d] + r0 * n, n * rows, o.field[KWB_REC_UX + d] + r0 * n)))
+        return rc;
     if (want(KWB_REC_P_MAX) && (rc = get32(gd.pmax, n, o.field[KWB_REC_P_MAX]))) return rc;
     if (want(KWB_REC_P_MIN) && (rc = get32(gd.pmin, n, o.field[KWB_REC_P_MIN]))) return rc;
     if (want(KWB_REC_P_FINAL) && (rc = get32(gd.pfinal, n, o.field[KWB_REC_P_FINAL]))) return rc;
@@ -1753,6 +1808,42 @@ int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) {
   }
   return KWB_OK;
 }
+
+// Time-series rows [r0, r1) of every recorded series into the caller's arrays, on stream cs
+// (ordered after the steps that wrote them by the caller).  Series rows are written once, by the
+// step of the same index, and post-loop filters are not pending (streamable).
+static int copy_series_rows(kwb_sim *S, kwb_outputs *out, long long r0, long long r1, cudaStream_t cs) {
+  for (size_t g = 0; g < S->groups.size(); ++g) {
+    const GroupHost &G = S->groups[g];
+    kwb_group_outputs &o = out->groups[g];
+    const long long n = G.n;
+    if (G.spec.cartesian || n == 0) continue;
+    const GroupDev &gd = G.dev;
+    const long long a = std::min(r0, gd.nt_alloc), b = std::min(r1, gd.nt_alloc);
+    if (b <= a) continue;
+    const float *src[4] = {gd.ser_p, gd.ser_u[0], gd.ser_u[1], gd.ser_u[2]};
+    const int fld[4] = {KWB_REC_P, KWB_REC_UX, KWB_REC_UY, KWB_REC_UZ};
+    for (int k = 0; k < 4; ++k) {
+      if (!(G.spec.record_mask & (1u << fld[k])) || !o.field[fld[k]] || !src[k]) continue;
+      const int rc = read_f32_as_f64(S->ctx, cs, src[k] + a * n, (b - a) * n, o.field[fld[k]] + a * n);
+      if (rc) return rc;
+    }
+  }
+  return KWB_OK;
+}
+
+// kwb_solve streams the time series back while the loop runs: no progress callback, no time
+// reversal, no elastic solver and no post-loop filters (which rewrite the series at the end).
+static bool series_streamable(const kwb_sim *S, const kwb_outputs *out) {
+  if (!out || !out->groups || S->progress || S->tr || S->h.elastic) return false;
+  for (const GroupHost &G : S->groups)
+    if (!G.filt_sin.empty()) return false;
+  return true;
+}
+
+extern "C" {
+
+int kwb_sim_read_outputs(kwb_sim *S, kwb_outputs *out) { return read_outputs_from(S, out, 0); }
 
 void kwb_sim_destroy(kwb_sim *S) {
   if (!S) return;
@@ -1795,12 +1886,58 @@ int kwb_sim_info(const kwb_sim *S, int64_t *device_bytes, int32_t *launches_per_
   return KWB_OK;
 }
 
+// The rest of the time loop in blocks of kSolveBlock steps: while block i runs, the time-series
+// rows of block i - 1 (at first, of the steps already done) are copied to the caller on a second
+// stream, so only the last block's rows and the aggregates are read after the loop.
+constexpr long long kSolveBlock = 8 * KWB_CHUNK_STEPS;
+
+int kwb_sim_finish(kwb_sim *S, kwb_outputs *out) {
+  if (!S || !out) return KWB_E_INVALID;
+  kwb_ctx *ctx = S->ctx;
+  CU(cudaSetDevice(ctx->device));
+  if (!series_streamable(S, out)) {
+    const int rc = kwb_sim_advance(S, S->Nt_loop - S->steps_done);
+    return rc ? rc : read_outputs_from(S, out, 0);
+  }
+  cudaStream_t cs = nullptr;
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  int rc = KWB_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(done[0], S->stream);  // the steps already done
+  if (e != cudaSuccess) rc = set_err(ctx, KWB_E_DEVICE, "CUDA error %s at solve streams", cudaGetErrorString(e));
+  long long rows = 0;
+  for (int i = 0; !rc && S->steps_done < S->Nt_loop; ++i) {
+    const long long s = S->steps_done;
+    if ((rc = kwb_sim_advance(S, std::min(kSolveBlock, S->Nt_loop - s)))) break;
+    if ((e = cudaEventRecord(done[(i + 1) & 1], S->stream)) != cudaSuccess) {
+      rc = set_err(ctx, KWB_E_DEVICE, "CUDA error %s at solve event", cudaGetErrorString(e));
+      break;
+    }
+    if (s > rows) {  // rows [rows, s) are final once the previous block has completed
+      if ((e = cudaStreamWaitEvent(cs, done[i & 1], 0)) != cudaSuccess) {
+        rc = set_err(ctx, KWB_E_DEVICE, "CUDA error %s at solve wait", cudaGetErrorString(e));
+        break;
+      }
+      if ((rc = copy_series_rows(S, out, rows, s, cs))) break;
+      rows = s;
+    }
+  }
+  if (!rc) rc = read_outputs_from(S, out, rows);
+  if (cs) {
+    cudaStreamSynchronize(cs);
+    cudaStreamDestroy(cs);
+  }
+  for (cudaEvent_t ev : done)
+    if (ev) cudaEventDestroy(ev);
+  return rc;
+}
+
 int kwb_solve(kwb_ctx *ctx, const kwb_problem *P, kwb_outputs *out) {
   kwb_sim *S = nullptr;
   int rc = kwb_sim_create(ctx, P, &S);
   if (rc) return rc;
-  rc = kwb_sim_advance(S, S->Nt_loop);
-  if (!rc) rc = kwb_sim_read_outputs(S, out);
+  rc = kwb_sim_finish(S, out);
   kwb_sim_destroy(S);
   return rc;
 }

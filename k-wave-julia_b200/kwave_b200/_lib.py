@@ -157,6 +157,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         lib.kwb_sim_sync.argtypes = [vp]
         lib.kwb_sim_read_outputs.restype = C.c_int
         lib.kwb_sim_read_outputs.argtypes = [vp, C.POINTER(Outputs)]
+        lib.kwb_sim_finish.restype = C.c_int
+        lib.kwb_sim_finish.argtypes = [vp, C.POINTER(Outputs)]
         lib.kwb_sim_read_pressure.restype = C.c_int
         lib.kwb_sim_read_pressure.argtypes = [vp, C.POINTER(C.c_float)]
         lib.kwb_sim_destroy.restype = None

@@ -556,6 +556,14 @@ class Simulation:
         self._chk(self.ctx.lib.kwb_sim_read_outputs(self.handle, C.byref(O)))
         return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt)
 
+    def finish(self) -> SimulationOutput:
+        """Run the remaining steps and return the outputs (``advance`` to Nt, then ``outputs``),
+        with the recorded time series copied back block by block while later steps run
+        (kwb_sim_finish)."""
+        O, outs, arrays, pfull = _alloc_outputs(self.ctx, self.b, self.kgrid)
+        self._chk(self.ctx.lib.kwb_sim_finish(self.handle, C.byref(O)))
+        return _collect(self.b, arrays, pfull, self.sensor, self.kgrid, self.Nt)
+
     def profile(self, steps: int) -> list:
         kt = _lib.KernelTimes()
         self._chk(self.ctx.lib.kwb_sim_profile(self.handle, int(steps), C.byref(kt)))

@@ -344,6 +344,23 @@ def test_graph_replay_matches_eager_chunks(kb, wl):
     assert np.array_equal(a.outputs()["p_max"], b.outputs()["p_max"])
 
 
+def test_uneven_advances_then_graph_chunks(kb, wl):
+    """Steps launched one by one (a count that is not a multiple of the 32-step graph chunk) and
+    graph chunks afterwards continue from the right step: the recorded series of 10 + 45 + 3 + 42
+    steps equals that of one advance of 100."""
+    case = wl.c2(n=96, Nt=100, record=("p", "p_max"))
+    g, m, s, sen, kw = case.to_api()
+    a = kb.Simulation(g, m, s, sen, **kw)
+    a.advance(100)
+    b = kb.Simulation(g, m, s, sen, **kw)
+    for k in (10, 45, 3, 42):
+        b.advance(k)
+    assert a.steps_done == b.steps_done == 100
+    oa, ob = a.outputs(), b.outputs()
+    for k in ("p", "p_max"):
+        assert np.array_equal(oa[k], ob[k]), k
+
+
 def test_progress_callback_sees_every_step(kb):
     n = 32
     g = kb.KWaveGrid(n, 1e-4, n, 1e-4)
@@ -384,6 +401,31 @@ def test_tiled_tma_staging_matches_cp_async(kb, monkeypatch, shape):
     assert set(out["1"].data) == set(out["0"].data) == {"p_final", "p_max", "p_rms"}
     for k in out["0"].data:
         assert np.array_equal(np.asarray(out["1"][k]), np.asarray(out["0"][k])), (shape, k)
+
+
+def test_finish_streams_the_series(kb):
+    """kwb_sim_finish (Simulation.finish; kwb_solve runs it) copies the recorded time series back
+    in blocks of 256 steps while later steps run: outputs bit-identical to advance + outputs, also
+    when some steps were advanced before, and through kspace_first_order.  (Runs with post-loop
+    filters are read after the loop; test_post_filters_on_the_device covers them.)"""
+    case = _p0_case((128, 96), 7, Nt=700, pml=8, record=("p", "p_max", "p_rms", "p_final"))
+    g, m, s, sen, kw = case.to_api()
+    outs = []
+    for pre in (None, 0, 300, 700):
+        sim = kb.Simulation(g, m, s, sen, **kw)
+        if pre is None:
+            sim.advance(sim.Nt)
+            outs.append(sim.outputs())
+        else:
+            sim.advance(pre)
+            outs.append(sim.finish())
+        sim.close()
+    outs.append(run_gpu(case))
+    for o in outs[1:]:
+        assert set(o.data) == set(outs[0].data)
+        for k in outs[0].data:
+            assert np.array_equal(np.asarray(o[k]), np.asarray(outs[0][k])), k
+    assert_parity(outs[0], run_oracle(case), TOL_L2, TOL_MAX)
 
 
 def test_bounded_tile_wait_reports_an_error(kb, monkeypatch):
