@@ -124,14 +124,23 @@ int read_f32_as_f64(kwb_ctx *ctx, cudaStream_t st, const float *src, long long c
   return KWB_OK;
 }
 
-// Julia's mean() sums pairwise; a pairwise sum keeps c_ref at FP64 round-off as well.
-double pairwise_sum(const double *x, long long n) {
+// Julia's mean() sums pairwise; a pairwise sum keeps c_ref at FP64 round-off as well.  The top
+// `par` levels of the same halving tree run on separate threads (the sum is the same, bit for
+// bit, as the sequential recursion).
+double pairwise_sum(const double *x, long long n, int par = 0) {
   if (n <= 128) {
     double s = 0.0;
     for (long long i = 0; i < n; ++i) s += x[i];
     return s;
   }
   const long long h = n / 2;
+  if (par > 0 && n >= (1LL << 20)) {
+    double left = 0.0;
+    std::thread t([&] { left = pairwise_sum(x, h, par - 1); });
+    const double right = pairwise_sum(x + h, n - h, par - 1);
+    t.join();
+    return left + right;
+  }
   return pairwise_sum(x, h) + pairwise_sum(x + h, n - h);
 }
 
@@ -711,8 +720,6 @@ size_t estimate_device_bytes(const kwb_problem *P) {
     // FP64 staging during set-up (released once the simulation is created)
     if (c_arr || r_arr || b_arr || P->p0.count)
       need += (size_t)nvox * 8 * (((nonlinear && b_arr && r_arr) ? 2 : 1) + ((P->row_major && D > 1) ? 1 : 0));
-    // the cluster plane pass's multiplier relayout copies the table once during set-up
-    if (D == 3 && fast_plane_size((int)N[1], (int)N[2])) need += (size_t)nspec * 4;
   }
   for (int g = 0; g < P->n_groups; ++g) {
     const kwb_sensor_group &G = P->groups[g];
@@ -1007,7 +1014,7 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
   const double r_s = P->rho0.count ? P->rho0.data[0] : 1.0;
   // (in memory order: for row-major input the summation order differs from the reference's
   // column-major one, which changes c_ref only at FP64 round-off)
-  const double c_ref = c_arr ? pairwise_sum(P->c0.data, nvox) / (double)nvox : c_s;
+  const double c_ref = c_arr ? pairwise_sum(P->c0.data, nvox, 4) / (double)nvox : c_s;
   const bool absorbing = P->alpha_mode != KWB_NO_ABSORPTION;
   const bool nonlinear = P->BonA.count > 0;
   h.nonlinear = nonlinear;
@@ -1294,20 +1301,23 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     const char *fx = getenv("KWB_FUSE_XEOS");
     h.fuse_xeos = (h.fast & 3) == 3 && D >= 2 && !h.dispersion && fast_size(h.N[0]) && !(fx && strcmp(fx, "0") == 0);
   }
+  // The EOS multiplier: allocated here, built once the FFT schedule is known, since the plane
+  // pass's slot-major variants read it in their own layout (the tuner's timing launches only
+  // need the buffer).
+  int *slot_ky = nullptr, *slot_kz = nullptr;
   if (!h.elastic) {
     float *Mt, *M2 = nullptr;
     CU(M.alloc(&Mt, h.nspec));
     if (h.dispersion) CU(M.alloc(&M2, h.nspec));
-    int *slot_ky = nullptr;
     if (h.plane) {
-      std::vector<int> ky(h.N[1]);
+      std::vector<int> ky(h.N[1]), kz(h.N[2]);
       fast_plane_slot_ky(h.N[1], ky.data());
+      fast_plane_slot_kz(h.N[2], kz.data());
       CU(M.alloc(&slot_ky, h.N[1]));
+      CU(M.alloc(&slot_kz, h.N[2]));
       if ((rc = upload(ctx, slot_ky, ky.data(), ky.size() * sizeof(int), st))) return rc;
+      if ((rc = upload(ctx, slot_kz, kz.data(), kz.size() * sizeof(int), st))) return rc;
     }
-    const double d3[3] = {P->d[0], D > 1 ? P->d[1] : 1.0, D > 2 ? P->d[2] : 1.0};
-    CU(build_eos_multiplier(Mt, M2, h.N, d3, c_ref, P->dt, c_arr ? 1.0 : c_s * c_s, absorbing, tau,
-                            eta, y, slot_ky, st));
     h.M = Mt;
     h.M2 = M2;
   }
@@ -1568,13 +1578,13 @@ int kwb_sim_create(kwb_ctx *ctx, const kwb_problem *P, kwb_sim **out) {
     if ((rc = choose_schedule(S.get(), h, st))) return rc;
     CU(prime_attributes(h));
   }
-  if (h.plane && fast_plane_slot_major(h)) {
-    // the slot-major plane pass reads its multiplier as [kx][slot][k_z in register order]
-    TempBuf tmp(st, ctx->pool);
-    float *Mk;
-    CU(tmp.alloc(&Mk, h.nspec));
-    CU(cudaMemcpyAsync(Mk, h.M, h.nspec * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    CU(fast_plane_relayout(const_cast<float *>(h.M), Mk, h.n1, st));
+  if (!h.elastic) {
+    // [kz][ky][kx]; with the plane pass [kx][kz][slot], or [kx][slot][k_z in register order]
+    // for its slot-major variants
+    const double d3[3] = {P->d[0], D > 1 ? P->d[1] : 1.0, D > 2 ? P->d[2] : 1.0};
+    CU(build_eos_multiplier(const_cast<float *>(h.M), const_cast<float *>(h.M2), h.N, d3, c_ref, P->dt,
+                            c_arr ? 1.0 : c_s * c_s, absorbing, tau, eta, y, h.plane ? slot_ky : nullptr,
+                            fast_plane_slot_major(h) ? slot_kz : nullptr, st));
   }
 
   slog.mark("schedule");

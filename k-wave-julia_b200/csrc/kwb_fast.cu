@@ -76,10 +76,10 @@ void fast_plane_slot_ky(int Ny, int *ky) {
   using F = fast::PlaneFY;
   for (int s = 0; s < Ny; ++s) ky[s] = F::k_of(s % F::G, s / F::G);
 }
-cudaError_t fast_plane_relayout(float *M, const float *M_kz_slot, int n1, cudaStream_t st) {
-  const long long total = (long long)n1 * 256 * 256;
-  fast::k_plane_m_cols<fast::PlaneFY><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(M, M_kz_slot, total);
-  return cudaGetLastError();
+// Register position j = t + 32 idx of the slot-major plane pass's z transform -> k_z.
+void fast_plane_slot_kz(int Nz, int *kz) {
+  using F = fast::PlaneFY;
+  for (int j = 0; j < Nz; ++j) kz[j] = F::k_of(j % 32, j / 32);
 }
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st) {
   (void)d_sim;

@@ -1692,7 +1692,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 // two cluster barriers, so nothing else orders the z step.  Rows are read from and written to
 // the plane directly (lane t holds x[t + 32 r]: coalesced 256-byte row segments).  The multiplier
 // is laid out [kx][slot][j] with k_z = F::k_of(j % 32, j / 32), so a line's 256 values are
-// contiguous (fast_plane_relayout).
+// contiguous (the table builder writes that layout when this variant runs).
 template <class F, int CL, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_plane_cols(const __grid_constant__ SimDev S, long long step_s) {
@@ -1773,18 +1773,6 @@ __global__ void __launch_bounds__(THREADS, MINB)
   }
 }
 
-// Multiplier of the slot-major plane pass, [kx][slot][j] with k_z = F::k_of(j % 32, j / 32), from
-// the [kx][k_z][slot] layout the table builder writes.
-template <class F>
-__global__ void k_plane_m_cols(float *__restrict__ out, const float *__restrict__ in, long long total) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  constexpr int N = F::N;
-  const int j = (int)(i % N), s = (int)((i / N) % N);
-  const long long kx = i / ((long long)N * N);
-  const int kz = F::k_of(j % 32, j / 32);
-  out[i] = in[(kx * N + kz) * N + s];
-}
 
 // ------------------------------------------------------------------------------------------
 // dispatch

@@ -346,16 +346,16 @@ bool fast_plane_size(int Ny, int Nz);
 bool fast_plane_available();
 #define KWB_PLANE_VARIANTS 6  // cluster plane-pass variants (kwb_fast_impl.cuh PlaneVariant)
 int fast_plane_variants(int *ids = nullptr);
-// The chosen plane-pass variant wants its multiplier slot-major (fast_plane_relayout from the
-// [kx][k_z][slot] table).
+// The chosen plane-pass variant wants its multiplier slot-major ([kx][slot][j], k_z of j from
+// fast_plane_slot_kz).
 bool fast_plane_slot_major(const SimDev &h);
+void fast_plane_slot_kz(int Nz, int *kz);
 cudaError_t fast_plane_prime();
 // Tensor maps of the fields a strided register line pass stages (p, rho0, u_d, rho_d), boxes of
 // `cols` columns x N / k positions along `axis` (the smallest k with N / k <= 256 dividing N);
 // false when the driver's encoder is unavailable or rejects a map (the pass then stages by
 // 16-byte cp.async).
 bool encode_strided_maps(SimDev &h, int axis, int cols);
-cudaError_t fast_plane_relayout(float *M, const float *M_kz_slot, int n1, cudaStream_t st);
 void fast_plane_slot_ky(int Ny, int *ky);
 cudaError_t fast_plane(const SimDev *d_sim, const SimDev &h, long long s, cudaStream_t st);
 
@@ -415,7 +415,7 @@ cudaError_t build_pml_deficit(float *out, int N, int pml_size, double alpha, dou
 cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const double d[3],
                                  double c_ref, double dt, double c_sq_fold, int absorbing,
                                  double tau, double eta, double y, const int *slot_ky,
-                                 cudaStream_t st);
+                                 const int *slot_kz, cudaStream_t st);
 // Reorder a row-major grid array (NumPy order) into column-major (x fastest); ndim 2 or 3.
 cudaError_t transpose_to_column_major(double *out, const double *in, int ndim, const int N[3],
                                       cudaStream_t st);

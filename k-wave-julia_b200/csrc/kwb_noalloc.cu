@@ -180,7 +180,7 @@ extern "C" int kwb_eos_pressure_noalloc(int device, int32_t ndim, const int64_t 
   }
   for (int a = 0; a < ndim && e == cudaSuccess; ++a) e = build_twiddles(const_cast<float2 *>(h.tw[a]), h.N[a], st);
   if (e == cudaSuccess)
-    e = build_eos_multiplier(const_cast<float *>(h.M), nullptr, h.N, d3, c_ref, dt, csq_fold, absorbing, tau, 0.0, y, nullptr, st);
+    e = build_eos_multiplier(const_cast<float *>(h.M), nullptr, h.N, d3, c_ref, dt, csq_fold, absorbing, tau, 0.0, y, nullptr, nullptr, st);
   const SimDev *d_sim = reinterpret_cast<const SimDev *>(base + kOffSim);
   if (e == cudaSuccess) e = launch_eos_x_fwd(d_sim, h, 0, st);
   if (e == cudaSuccess && ndim == 2) e = launch_spec_pass(d_sim, h, 1, KWB_SPEC_FWD_MUL_INV, 0, st);

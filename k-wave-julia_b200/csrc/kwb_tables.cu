@@ -54,17 +54,22 @@ __global__ void k_build_pml_deficit(float *out, int N, int pml_size, double alph
 }
 
 // Layouts: [k_z][k_y][k_x] (slot_ky == nullptr) or, for the cluster plane pass,
-// [k_x][k_z][slot] with k_y = slot_ky[slot].
+// [k_x][k_z][slot] with k_y = slot_ky[slot], or, for its slot-major variant (slot_kz given),
+// [k_x][slot][j] with k_z = slot_kz[j].
 __global__ void k_build_eos_multiplier(float *M, float *M2, int Nx, int Ny, int Nz, double dx,
                                        double dy, double dz, double c_ref, double dt,
                                        double c_sq_fold, int absorbing, double tau, double eta,
-                                       double y, const int *slot_ky) {
+                                       double y, const int *slot_ky, const int *slot_kz) {
   const int n1 = Nx / 2 + 1;
   const long long total = (long long)n1 * Ny * Nz;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= total) return;
   int kx, ky, kz;
-  if (slot_ky) {
+  if (slot_kz) {
+    kz = slot_kz[(int)(idx % Nz)];
+    ky = slot_ky[(int)((idx / Nz) % Ny)];
+    kx = (int)(idx / ((long long)Ny * Nz));
+  } else if (slot_ky) {
     ky = slot_ky[(int)(idx % Ny)];
     kz = (int)((idx / Ny) % Nz);
     kx = (int)(idx / ((long long)Ny * Nz));
@@ -153,11 +158,11 @@ cudaError_t build_pml_deficit(float *out, int N, int pml_size, double alpha, dou
 cudaError_t build_eos_multiplier(float *M, float *M2, const int N[3], const double d[3],
                                  double c_ref, double dt, double c_sq_fold, int absorbing,
                                  double tau, double eta, double y, const int *slot_ky,
-                                 cudaStream_t st) {
+                                 const int *slot_kz, cudaStream_t st) {
   const long long total = (long long)(N[0] / 2 + 1) * N[1] * N[2];
   k_build_eos_multiplier<<<blocks(total, 256), 256, 0, st>>>(M, M2, N[0], N[1], N[2], d[0],
                                                              d[1], d[2], c_ref, dt, c_sq_fold,
-                                                             absorbing, tau, eta, y, slot_ky);
+                                                             absorbing, tau, eta, y, slot_ky, slot_kz);
   return cudaGetLastError();
 }
 cudaError_t transpose_to_column_major(double *out, const double *in, int ndim, const int N[3],
