@@ -10,9 +10,9 @@
 //   * Stockham passes (other lengths): the radix order of each axis's plan, the complex lines per
 //     tile, and the threads per CTA of the line passes.
 // Each candidate runs on the simulation's own buffers before its initial conditions are set
-// (sensors, sources and time reversal are switched off in the timing descriptor), one warm-up
-// launch then three timed with CUDA events; a pass's choice does not depend on another's, so the
-// passes are tuned one at a time.  Every candidate computes the same transform: the tile shape
+// (sensors, sources and time reversal are switched off in the timing descriptor): one warm-up
+// time step, then three timed with CUDA events, so that a candidate is judged by the step it
+// gives; the passes are tuned one at a time, each with the others at their current choice.  Every candidate computes the same transform: the tile shape
 // and thread count leave the arithmetic of each line unchanged, so results are bit-identical
 // whatever is picked -- a simulation gives the same fields alone, tuned, and in a batch, which
 // keeps the heuristic.  A different radix order only reorders FP32 rounding; it is explored
@@ -198,10 +198,29 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
   if (e != cudaSuccess) return e;
   const int D = h.ndim;
   const SimDev *d = d_scratch;
+  // Every candidate is timed on whole time steps (the step's passes launched as the simulation
+  // launches them, each waiting on its predecessor by programmatic dependent launch), not on its
+  // own pass alone: a pass's tile shape also changes how its launch overlaps its neighbours'.
+  auto step = [&]() -> cudaError_t {
+    cudaError_t e;
+    for (int a : {1, 2, 0})
+      if (a < D && (e = launch_line_pass(d, t, a, KWB_MODE_STEP, 0, st)) != cudaSuccess) return e;
+    if (!t.fuse_xeos && (e = launch_eos_x_fwd(d, t, 0, st)) != cudaSuccess) return e;
+    if (D == 2) {
+      if ((e = launch_spec_pass(d, t, 1, KWB_SPEC_FWD_MUL_INV, 0, st)) != cudaSuccess) return e;
+    } else if (D == 3 && t.plane) {
+      if ((e = fast_plane(d, t, 0, st)) != cudaSuccess) return e;
+    } else if (D == 3) {
+      if ((e = launch_spec_pass(d, t, 1, KWB_SPEC_FWD, 0, st)) != cudaSuccess) return e;
+      if ((e = launch_spec_pass(d, t, 2, KWB_SPEC_FWD_MUL_INV, 0, st)) != cudaSuccess) return e;
+      if ((e = launch_spec_pass(d, t, 1, KWB_SPEC_INV, 0, st)) != cudaSuccess) return e;
+    }
+    return launch_eos_x_inv(d, t, 0, st);
+  };
 
   // line passes (the x pass carries the EOS x R2C when fused)
   for (int a = 0; a < D; ++a) {
-    auto go = [&, a] { return launch_line_pass(d, t, a, KWB_MODE_STEP, 0, st); };
+    auto go = step;
     if (line_is_fast(t, a)) {
       T.choose("line_tile", 3, [&, a](int i) { t.tile_var[KWB_SLOT_LINE0 + a] = (signed char)i; }, go);
       // tiles staged by TMA copies or by 16-byte cp.async (unless KWB_TILE_TMA fixes it)
@@ -238,15 +257,12 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
     if (eos_is_fast(t)) {
       if (!t.fuse_xeos)
         T.choose("eos_fwd_tile", 3, [&](int i) { t.tile_var[KWB_SLOT_EOS_FWD] = (signed char)i; },
-                 [&] { return launch_eos_x_fwd(d, t, 0, st); });
+                 step);
       T.choose("eos_inv_tile", 3, [&](int i) { t.tile_var[KWB_SLOT_EOS_INV] = (signed char)i; },
-               [&] { return launch_eos_x_inv(d, t, 0, st); });
+               step);
     } else {
       const std::vector<int> Ls = l_candidates(fft_len(t.plan[0]), t.L_eosx, (t.N[1] + 1) / 2, t.dispersion, true);
-      T.choose("eos_L", (int)Ls.size(), [&](int i) { t.L_eosx = Ls[i]; }, [&] {
-        cudaError_t r = launch_eos_x_fwd(d, t, 0, st);
-        return r == cudaSuccess ? launch_eos_x_inv(d, t, 0, st) : r;
-      });
+      T.choose("eos_L", (int)Ls.size(), [&](int i) { t.L_eosx = Ls[i]; }, step);
     }
   }
 
@@ -258,12 +274,12 @@ cudaError_t tune_schedule(SimDev &h, SimDev *d_scratch, cudaStream_t st, int pic
     int ids[KWB_PLANE_VARIANTS];
     const int nv = fast_plane_variants(ids);
     T.choose("plane", nv > 1 ? nv : 0, [&](int i) { t.tile_var[KWB_SLOT_PLANE] = (signed char)ids[i]; },
-             [&] { return fast_plane(d, t, 0, st); });
+             step);
   }
   // spectrum passes along y and z
   if (!t.plane) {
     for (int a = 1; a < D; ++a) {
-      auto go = [&, a] { return launch_spec_pass(d, t, a, KWB_SPEC_FWD_MUL_INV, 0, st); };
+      auto go = step;
       if (spec_is_fast(t, a)) {
         T.choose("spec_tile", 3, [&, a](int i) { t.tile_var[KWB_SLOT_SPEC1 + a - 1] = (signed char)i; }, go);
       } else {
